@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark of the Siddon forward projector A and its adjoint A^T on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cone256]
+
+A step is one forward + adjoint pair over the whole scan of the workload
+(default cone256: 256^3 volume at 0.5 mm, 360 views of 512x384 cells,
+70,778,880 rays; seeded synthetic ellipsoid phantom).  The metric is
+GRays/s fwd+adj = rays / (t_fwd + t_adj) / 1e9.
+
+ours (default): device-resident timing with CUDA events on the launching
+stream, W untimed warm-up steps, then K timed steps; L2 is flushed (a
+512 MiB write) before every timed step and the flush is not timed.  With
+N > 1 (torchrun, one process per GPU) every rank projects its own full scan
+(independent scans, weak scaling, no collective on the data path) and the
+time is the max over ranks.  Rank 0 prints one JSON line that also holds:
+  roofline      dominant kernel: algorithmic bytes / mean launch time vs the
+                measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline  the CPU port of the reference's torch path (oracle/) on this
+                host's cores, on a bounded sample of views (N = 1 only)
+  e2e           the same metric through the public module API with pinned
+                host buffers, H2D of each step's inputs and D2H of its outputs
+                inside the timed region
+  clocks        nvidia-smi SM clock / throttle reasons sampled while timing
+
+reference: times the reference's CPU projector (the oracle's port of its
+torch path) on the host cores, rank 0 only, K steps each a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic segment counts (sum over rays of in-volume Siddon segments),
+# frozen from the FP64 oracle: `python oracle/count_segments.py <workload>`.
+SEGMENTS = {
+    "fan256": 45_364_441,
+    "cone256": None,  # filled below once counted
+}
+METRIC = "GRays/s fwd+adj"
+L2_FLUSH_BYTES = 512 << 20
+
+
+# --------------------------------------------------------------------------- helpers
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def algorithmic_bytes(workload, n_ray):
+    """Per launch, fwd or adj: 4 B per in-volume segment (one voxel read or
+    one accumulation) + 4 B per ray (sinogram write or read)."""
+    seg = SEGMENTS.get(workload)
+    if seg is None:
+        return None, None
+    return 4 * seg + 4 * n_ray, seg
+
+
+class ClockSampler:
+    """nvidia-smi SM clock and throttle reasons, sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif args.impl == "ours":
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- CPU legs
+def cpu_threads():
+    n = len(os.sched_getaffinity(0))
+    return max(1, min(n, 64))
+
+
+class CpuCase:
+    """Host copies of a workload's geometry and phantom for the CPU legs."""
+
+    def __init__(self, w, src=None, dst=None, M=None, b=None, vol=None):
+        from oracle import oracle as O
+        if src is None:
+            src, dst, M, b = w.geometry()
+        self.w = w
+        self.src = np.ascontiguousarray(src.cpu().numpy() if torch.is_tensor(src) else src)
+        self.dst = np.ascontiguousarray(dst.cpu().numpy() if torch.is_tensor(dst) else dst)
+        self.Mi = O.minv(M.cpu().numpy() if torch.is_tensor(M) else M)
+        self.b = np.ascontiguousarray(b.cpu().numpy() if torch.is_tensor(b) else b)
+        if vol is None:
+            vol = w.phantom(device="cuda" if torch.cuda.is_available() else "cpu")
+        self.vol = np.ascontiguousarray(vol.cpu().numpy() if torch.is_tensor(vol) else vol)
+        self.per_view = w.n_ray // w.n_view
+
+    def rate(self, views, threads):
+        """Rays/s of the oracle's port of the reference CPU path (intersections
+        + sort + segment sum, then the scatter adjoint) on the given views."""
+        from oracle import oracle as O
+        O.set_threads(threads)
+        idx = np.concatenate([np.arange(v * self.per_view, (v + 1) * self.per_view) for v in views])
+        s, d = self.src[idx], self.dst[idx]
+        y = np.random.default_rng(0).random(idx.size).astype(np.float32)
+        t0 = time.perf_counter()
+        O.fwd_otf_torch(self.vol, self.Mi, self.b, s, d)
+        O.back_otf_torch(y, self.Mi, self.b, s, d, self.vol.shape)
+        dt = time.perf_counter() - t0
+        return idx.size / dt, idx.size, dt
+
+
+def cpu_baseline(case, target_s=15.0):
+    w = case.w
+    threads = cpu_threads()
+    rate, n, dt = case.rate([0], threads)  # calibration: one view
+    n_views = int(max(1, min(w.n_view, math.floor(target_s * rate / case.per_view))))
+    views = [int(round(i * w.n_view / n_views)) % w.n_view for i in range(n_views)]
+    rate, n, dt = case.rate(views, threads)
+    return {"value": rate / 1e9, "unit": "GRays/s", "cores": threads, "kind": "port",
+            "sample": f"{n_views} of {w.n_view} views evenly spaced ({n} rays, {dt:.1f} s fwd+adj), "
+                      "extrapolated linearly (rays are independent)"}
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU projector on this host's cores (rank 0 only)."""
+    from ct_laboratory_b200.workloads import WORKLOADS
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    case = CpuCase(w)
+    threads = cpu_threads()
+    rate, _, _ = case.rate([0], threads)
+    n_views = int(max(1, min(w.n_view, math.floor(args.ref_step_s * rate / case.per_view))))
+    for i in range(args.warmup):
+        case.rate([i % w.n_view], threads)
+    rays, secs = 0, 0.0
+    for k in range(args.steps):
+        vs = [(k * 7 + j * max(1, w.n_view // n_views)) % w.n_view for j in range(n_views)]
+        r, n, dt = case.rate(vs, threads)
+        rays += n
+        secs += dt
+    value = rays / secs / 1e9
+    out = {"metric": METRIC, "value": value, "unit": "GRays/s", "impl": "reference", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": w.name, "n_ray": w.n_ray, "sample_views_per_step": n_views},
+           "cpu_baseline": {"value": value, "unit": "GRays/s", "cores": threads, "kind": "port",
+                            "sample": f"{n_views} views per step of {w.n_view}, rotating"},
+           "e2e": {"value": value, "unit": "GRays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# --------------------------------------------------------------------------- GPU leg
+def run_ours(args, world, rank, local):
+    from ct_laboratory_b200 import ConeBeam3DProjector, FanBeam2DProjector
+    import dataclasses
+
+    from ct_laboratory_b200.workloads import WORKLOADS
+    w = WORKLOADS[args.workload]
+    if args.views:
+        w = dataclasses.replace(w, n_view=args.views, name=f"{w.name}-v{args.views}")
+    dev = torch.device("cuda", local)
+    if w.name.startswith("cone"):
+        proj = ConeBeam3DProjector(*w.n, n_view=w.n_view, det_nx=w.det_nx, det_ny=w.det_ny, sid=w.sid, sdd=w.sdd,
+                                   det_spacing=w.pitch, voxel_size=w.voxel, device=dev, tile_rows=args.tile_rows)
+    else:
+        proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
+                                  pixel_size=w.pixel, device=dev)
+    n_ray = proj.src.shape[0]
+    x = w.phantom(device=dev)
+    y = torch.rand(n_ray, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    launches_per_step = 2
+
+    def fwd():
+        return proj.forward_project(x) if not w.name.startswith("cone") else _fwd3(proj, x)
+
+    def adj():
+        return proj.back_project(y)
+
+    with torch.no_grad():
+        for _ in range(args.warmup):
+            fwd()
+            adj()
+        torch.cuda.synchronize(dev)
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                ev[k][0].record(stream)
+                fwd()
+                ev[k][1].record(stream)
+                adj()
+                ev[k][2].record(stream)
+            torch.cuda.synchronize(dev)
+        barrier(world)
+    t_fwd = np.array([e[0].elapsed_time(e[1]) for e in ev])
+    t_adj = np.array([e[1].elapsed_time(e[2]) for e in ev])
+    total_ms = float((t_fwd + t_adj).sum())
+    total_ms = max_over_ranks(total_ms, world)
+    value = world * n_ray * args.steps / (total_ms / 1e3) / 1e9
+
+    peak, peak_src = peaks()
+    bytes_per_launch, seg = algorithmic_bytes(w.name, n_ray)
+    kern = {}
+    for name, t in (("forward", t_fwd), ("adjoint", t_adj)):
+        ms = float(t.mean())
+        ach = bytes_per_launch / (ms / 1e3) / 1e9 if bytes_per_launch else None
+        kern[name] = {"ms_mean": ms, "ms_min": float(t.min()), "achieved_gbs": ach,
+                      "frac": (ach / peak) if ach else None}
+    dom = max(kern, key=lambda k: kern[k]["ms_mean"])
+    traffic = load_traffic(w.name, dom)
+    roofline = {"bound": "hbm", "achieved": kern[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "segments": seg, "kernels": kern}
+
+    e2e = run_e2e(proj, x, y, args, dev, w) if args.e2e_steps > 0 else None
+    cpu = None
+    if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
+        cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s)
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "GRays/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": w.name, "n_ray": n_ray, "volume": list(w.n),
+                          "views": w.n_view, "rays_per_rank": n_ray, "l2": "flushed (512 MiB write) before each step",
+                          "tile_rows": args.tile_rows, "parallelism": f"independent scans x{world}"},
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+               "gpu_launches": launches_per_step * args.steps}
+        print(json.dumps(out))
+
+
+def _fwd3(proj, x):
+    return proj.forward_project(x)
+
+
+def run_e2e(proj, x, y, args, dev, w):
+    """Public API, host buffers: H2D of the volume and of the adjoint input,
+    D2H of the sinogram and of the back-projection, every step."""
+    x_h = x.cpu().pin_memory()
+    y_h = y.cpu().pin_memory()
+    sino_h = torch.empty(y.shape, dtype=torch.float32).pin_memory()
+    vol_h = torch.empty(x.shape, dtype=torch.float32).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        xd = x_h.to(dev, non_blocking=True)
+        s = proj(xd)
+        sino_h.copy_(s, non_blocking=True)
+        yd = y_h.to(dev, non_blocking=True)
+        v = proj.back_project(yd)
+        vol_h.copy_(v, non_blocking=True)
+
+    with torch.no_grad():
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.e2e_steps
+    n_ray = y.numel()
+    return {"value": n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
+            "h2d_bytes_per_step": int(x_h.numel() * 4 + y_h.numel() * 4),
+            "d2h_bytes_per_step": int(sino_h.numel() * 4 + vol_h.numel() * 4),
+            "api": "ConeBeam3DProjector.__call__ + .back_project" if w.name.startswith("cone")
+            else "FanBeam2DProjector.__call__ + .back_project"}
+
+
+def load_traffic(workload, kernel):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="cone256")
+    ap.add_argument("--tile-rows", type=int, default=32)
+    ap.add_argument("--views", type=int, default=0,
+                    help="override the workload's view count (smaller cases for profiler captures)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-baseline-s", type=float, default=15.0)
+    ap.add_argument("--ref-step-s", type=float, default=4.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,106 @@
+"""ctypes binding of libctlab_b200.so (the C ABI declared in include/ctlab_b200.h).
+
+The library is required: importing this module raises ImportError when it
+has not been built (``python -m ct_laboratory_b200.build``).  There is no
+Python or CPU fallback for any projector.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libctlab_b200.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        f"ct_laboratory_b200: native library {_LIB_PATH} is missing; build it with "
+        "`python -m ct_laboratory_b200.build` (nvcc, sm_100a)")
+
+lib = ctypes.CDLL(_LIB_PATH)
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+class RayTiling(ctypes.Structure):
+    """Mirror of ctlab_ray_tiling (include/ctlab_b200.h)."""
+
+    _fields_ = [("n_view", _I64), ("n_row", _I64), ("n_col", _I64), ("view_stride", _I64),
+                ("row_stride", _I64), ("col_stride", _I64), ("tile_rows", ctypes.c_int32),
+                ("block_threads", ctypes.c_int32)]
+
+
+_TP = ctypes.POINTER(RayTiling)
+
+# name -> argtypes (every entry point returns int)
+_SIGS = {
+    "ctlab_forward_project_3d_on_the_fly": [_P, _I64, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_back_project_3d_on_the_fly": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _P],
+    "ctlab_forward_project_3d_on_the_fly_ex": [_P, _I64, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _TP, _P],
+    "ctlab_back_project_3d_on_the_fly_ex": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P],
+    "ctlab_compute_intersections_3d": [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_forward_project_3d_tvals": [_P, _I64, _I64, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_back_project_3d_tvals": [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _P],
+    "ctlab_compress_tvals_3d": [_P, _I64, _I64, _P, _P, _F, _P, _P, _P, _P],
+    "ctlab_compress_tvals_3d_ex": [_P, _I64, _I64, _P, _P, _F, _P, _P, _P, _I, _P],
+    "ctlab_forward_project_3d_compressed": [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _I64, _P, _P, _I64, _P, _P, _P,
+                                            _P],
+    "ctlab_back_project_3d_compressed": [_P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I,
+                                         _P],
+    "ctlab_compute_intersections_2d": [_I64, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_forward_project_2d_tvals": [_P, _I64, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_back_project_2d_tvals": [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _P],
+    "ctlab_forward_project_2d_on_the_fly": [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P],
+    "ctlab_back_project_2d_on_the_fly": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _P],
+    "ctlab_forward_project_2d_siddon": [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _TP, _P],
+    "ctlab_back_project_2d_siddon": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P],
+    "ctlab_invert_matrix": [_P, _I, _P, _P, _P],
+}
+
+for _name, _args in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = ctypes.c_int
+
+lib.ctlab_last_error.restype = ctypes.c_char_p
+lib.ctlab_last_error.argtypes = []
+lib.ctlab_abi_version.restype = ctypes.c_int
+lib.ctlab_abi_version.argtypes = []
+
+ABI_VERSION = lib.ctlab_abi_version()
+
+
+def exported_symbols():
+    """Names of the C entry points this binding declares."""
+    return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version"]
+
+
+def call(name: str, *args) -> None:
+    """Invoke an entry point and raise RuntimeError on a non-zero status."""
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        msg = lib.ctlab_last_error().decode(errors="replace")
+        raise RuntimeError(f"{name} failed (status {rc}): {msg}")
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream_of(t: torch.Tensor):
+    """Raw handle of the current torch stream on t's device."""
+    return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def tiling(n_view, n_row, n_col, view_stride, row_stride, col_stride, tile_rows=32, block_threads=256):
+    return RayTiling(int(n_view), int(n_row), int(n_col), int(view_stride), int(row_stride), int(col_stride),
+                     int(tile_rows), int(block_threads))
+
+
+def tiling_ref(t):
+    return None if t is None else ctypes.byref(t)

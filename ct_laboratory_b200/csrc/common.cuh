@@ -1,0 +1,150 @@
+// common.cuh — shared helpers of the B200 Siddon kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+
+#include "ctlab_b200.h"
+
+namespace ctlab {
+
+// ----------------------------------------------------------------------------
+// Host-side status plumbing
+// ----------------------------------------------------------------------------
+
+// Records a printf-style message as the calling thread's last error and
+// returns `code`.
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+
+#define CTLAB_REQUIRE(cond, ...)                                  \
+    do {                                                          \
+        if (!(cond)) return ::ctlab::set_error(CTLAB_EINVAL, __VA_ARGS__); \
+    } while (0)
+
+#define CTLAB_CUDA_TRY(call)                                                              \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ::ctlab::set_error(CTLAB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// After a launch: report configuration errors without synchronising.
+inline int launch_status(const char* what) {
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(CTLAB_ECUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+    }
+    return CTLAB_OK;
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr int64_t kMaxGrid = 2147483647LL;
+
+// ----------------------------------------------------------------------------
+// Device helpers shared by every kernel.  Expressions the reference writes
+// as a*b + c (which nvcc contracts into fused multiply-adds) are written here
+// with explicit __fmaf_rn / __fmul_rn so the rounding is pinned and matches
+// the reference's kernels, e.g. apply_affine_inverse_3d
+// (ct_projector_3d.cu:21-36).
+// ----------------------------------------------------------------------------
+
+struct Affine3 {
+    float m[9];
+    float b[3];
+};
+
+struct Affine2 {
+    float m[4];
+    float b[2];
+};
+
+__device__ __forceinline__ Affine3 load_affine3(const float* __restrict__ M_inv, const float* __restrict__ b) {
+    Affine3 a;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) a.m[i] = __ldg(M_inv + i);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) a.b[i] = __ldg(b + i);
+    return a;
+}
+
+__device__ __forceinline__ Affine2 load_affine2(const float* __restrict__ M_inv, const float* __restrict__ b) {
+    Affine2 a;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a.m[i] = __ldg(M_inv + i);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) a.b[i] = __ldg(b + i);
+    return a;
+}
+
+// a*b + c*d the way nvcc contracts it when both products have one use: the
+// first product is fused, fma(a, b, c*d).  Set CTLAB_CONTRACT_FIRST=0 to fuse
+// the second instead.
+#ifndef CTLAB_CONTRACT_FIRST
+#define CTLAB_CONTRACT_FIRST 1
+#endif
+__device__ __forceinline__ float mad2(float a, float b, float c, float d) {
+#if CTLAB_CONTRACT_FIRST
+    return __fmaf_rn(a, b, __fmul_rn(c, d));
+#else
+    return __fmaf_rn(c, d, __fmul_rn(a, b));
+#endif
+}
+
+// x*x + y*y + z*z, left to right, contracted.
+__device__ __forceinline__ float sumsq3(float x, float y, float z) { return __fmaf_rn(z, z, mad2(x, x, y, y)); }
+__device__ __forceinline__ float sumsq2(float x, float y) { return mad2(x, x, y, y); }
+
+__device__ __forceinline__ void world_to_index3(const Affine3& A, float x, float y, float z, float& i, float& j,
+                                                float& k) {
+    float xs = __fsub_rn(x, A.b[0]), ys = __fsub_rn(y, A.b[1]), zs = __fsub_rn(z, A.b[2]);
+    i = __fmaf_rn(A.m[2], zs, mad2(A.m[0], xs, A.m[1], ys));
+    j = __fmaf_rn(A.m[5], zs, mad2(A.m[3], xs, A.m[4], ys));
+    k = __fmaf_rn(A.m[8], zs, mad2(A.m[6], xs, A.m[7], ys));
+}
+
+__device__ __forceinline__ void world_to_index2(const Affine2& A, float x, float y, float& r, float& c) {
+    float xs = __fsub_rn(x, A.b[0]), ys = __fsub_rn(y, A.b[1]);
+    r = mad2(A.m[0], xs, A.m[1], ys);
+    c = mad2(A.m[2], xs, A.m[3], ys);
+}
+
+// Plane parameter of plane coordinate p along one axis: (p - s) * inv, the
+// reciprocal-multiply form of collect_hits (ct_projector_3d.cu:866-868).
+__device__ __forceinline__ float plane_t(float p, float s, float inv) { return __fmul_rn(__fsub_rn(p, s), inv); }
+
+// Ray tiling resolved on the host into plain integers for the kernels.
+struct Tiling {
+    int64_t n_view, n_row, n_col;
+    int64_t view_stride, row_stride, col_stride;
+    int tile_rows, tile_cols;       // tile_rows * tile_cols == blockDim.x
+    int64_t tiles_r, tiles_c;       // tiles per view along rows / cols
+    int64_t n_blocks;               // n_view * tiles_r * tiles_c
+};
+
+// Validates `t` (may be NULL = flat) against n_ray and fills `out`.
+int resolve_tiling(const ctlab_ray_tiling* t, int64_t n_ray, Tiling& out);
+
+// Ray handled by this thread, or -1 when the thread's slot is outside the grid.
+__device__ __forceinline__ int64_t tile_ray(const Tiling& T) {
+    int64_t blk = blockIdx.x;
+    int64_t per_view = T.tiles_r * T.tiles_c;
+    int64_t view = blk / per_view;
+    int64_t rem = blk - view * per_view;
+    int64_t tr = rem / T.tiles_c;
+    int64_t tc = rem - tr * T.tiles_c;
+    int lane_r = threadIdx.x % T.tile_rows;
+    int lane_c = threadIdx.x / T.tile_rows;
+    int64_t row = tr * T.tile_rows + lane_r;
+    int64_t col = tc * T.tile_cols + lane_c;
+    if (row >= T.n_row || col >= T.n_col) return -1;
+    return view * T.view_stride + row * T.row_stride + col * T.col_stride;
+}
+
+}  // namespace ctlab

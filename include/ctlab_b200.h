@@ -1,0 +1,216 @@
+/*
+ * ctlab_b200.h — C ABI of the B200 Siddon projector (libctlab_b200.so).
+ *
+ * Every entry point takes raw device pointers, 64-bit sizes and a CUDA stream
+ * (passed as void*, i.e. a cudaStream_t; NULL means the legacy default
+ * stream), launches asynchronously on that stream and returns a status code.
+ * Nothing is allocated: the caller owns every buffer, outputs included.
+ * Errors never cross the ABI as exceptions; ctlab_last_error() returns the
+ * message of the calling thread's most recent failure.
+ *
+ * Data layouts are the reference's (ct_laboratory, src/ct_projector_*.cu):
+ *   volume   float32 [batch, n_x, n_y, n_z], C-contiguous (k fastest)
+ *   image    float32 [batch, n_row, n_col], C-contiguous
+ *   src, dst float32 [n_ray, 3] (3-D) or [n_ray, 2] (2-D), world coordinates
+ *   sinogram float32 [batch, n_ray]
+ *   M_inv    float32 [9] (3-D) or [4] (2-D), row-major inverse of the
+ *            voxel-index -> world matrix M;   b float32 [3] / [2].
+ *            Both live in device memory, exactly as the reference's kernels
+ *            take them (ct_projector_3d.cu:21-36).
+ *   tvals    float32 [n_ray, n_int], sorted plane parameters, +inf padded
+ *   t_uint16 uint16  [n_ray, n_int] delta-encoded tvals (stored by the
+ *            reference in a torch.int16 tensor), t_start / t_scale [n_ray].
+ *
+ * Adjoint entry points take `accumulate`: 0 zeroes `out` on the stream first
+ * (the reference returns torch::zeros-initialised volumes), 1 adds into it.
+ */
+#ifndef CTLAB_B200_H
+#define CTLAB_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTLAB_OK 0
+#define CTLAB_EINVAL 1  /* bad argument: null pointer, negative or oversized dimension */
+#define CTLAB_ECUDA 2   /* a CUDA runtime call or kernel launch failed */
+#define CTLAB_ETIMEOUT 3 /* a bounded device-side wait gave up */
+
+#define CTLAB_ABI_VERSION 1
+
+/* ABI version of the loaded library (CTLAB_ABI_VERSION). */
+int ctlab_abi_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* ctlab_last_error(void);
+
+/* M_inv = M^-1 for a row-major n x n matrix (n = 2 or 3) in device memory,
+ * computed on the stream by Gauss-Jordan elimination with partial pivoting.
+ * Replaces the torch.inverse(M) calls of the reference's wrappers
+ * (tomography/ct_projector_3d_cuda.py:42-48, ct_projector_2d_cuda.py:6-8)
+ * without a host synchronisation.  A singular or non-finite M yields NaN
+ * entries and, if `singular` is not NULL, *singular = 1 (device memory). */
+int ctlab_invert_matrix(const float* M, int n, float* M_inv, int* singular, void* stream);
+
+/*
+ * Ray tiling of a launch.  Rays are addressed as a grid
+ *     ray = view * view_stride + row * row_stride + col * col_stride
+ * with n_view x n_row x n_col entries (n_view*n_row*n_col must equal n_ray).
+ * One CTA covers `tile_rows` consecutive rows of (block_threads / tile_rows)
+ * columns of one view, and the lanes of a warp run along rows.  For a cone-
+ * beam scan ordered [view][det_v][det_u] (conebeam_projector_3d.py:84-94)
+ * rows = det_v, cols = det_u puts adjacent lanes on vertically adjacent
+ * detector cells, whose rays visit adjacent voxels of the k-fastest volume.
+ * A NULL tiling means a flat run: n_view = 1, n_row = n_ray, n_col = 1.
+ */
+typedef struct ctlab_ray_tiling {
+    int64_t n_view, n_row, n_col;
+    int64_t view_stride, row_stride, col_stride;
+    int32_t tile_rows;     /* 1..block_threads, divides block_threads; 0 = 32 */
+    int32_t block_threads; /* multiple of 32, <= 1024; 0 = 256 */
+} ctlab_ray_tiling;
+
+/* ---------------------------------------------------------------------- */
+/* 3-D, on the fly (no intersection table)                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces _C.forward_project_3d_on_the_fly_cuda (src/bindings.cpp:98;
+ * host wrapper src/ct_projector_3d.cu:1018-1049, kernel :902-1012).
+ * out[b, r] = sum over the ray's voxels of volume[b, voxel] * segment length. */
+int ctlab_forward_project_3d_on_the_fly(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
+                                        int64_t n_z, const float* src, const float* dst, int64_t n_ray,
+                                        const float* M_inv, const float* b, float* out, void* stream);
+
+/* Replaces _C.back_project_3d_on_the_fly_cuda (src/bindings.cpp:101;
+ * src/ct_projector_3d.cu:1051-1079): the exact adjoint of the above, by
+ * atomic scatter of sino[b, r] * segment length. */
+int ctlab_back_project_3d_on_the_fly(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                     const float* dst, const float* M_inv, const float* b, int64_t n_x,
+                                     int64_t n_y, int64_t n_z, float* out, int accumulate, void* stream);
+
+/* The two calls above with an explicit ray tiling (NULL = flat). */
+int ctlab_forward_project_3d_on_the_fly_ex(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
+                                           int64_t n_z, const float* src, const float* dst, int64_t n_ray,
+                                           const float* M_inv, const float* b, float* out,
+                                           const ctlab_ray_tiling* tiling, void* stream);
+int ctlab_back_project_3d_on_the_fly_ex(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                        const float* dst, const float* M_inv, const float* b, int64_t n_x,
+                                        int64_t n_y, int64_t n_z, float* out, int accumulate,
+                                        const ctlab_ray_tiling* tiling, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* 3-D, precomputed intersections                                          */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces _C.compute_intersections_3d (src/bindings.cpp:83;
+ * src/ct_projector_3d.cu:42-96, 381-401).  t_out is [n_ray, n_int] with
+ * n_int = (n_x+1)+(n_y+1)+(n_z+1): every x/y/z plane parameter in [0,1],
+ * ascending, then +inf. */
+int ctlab_compute_intersections_3d(int64_t n_x, int64_t n_y, int64_t n_z, const float* src, const float* dst,
+                                   int64_t n_ray, const float* M_inv, const float* b, float* t_out,
+                                   void* stream);
+
+/* Replaces _C.forward_project_3d_cuda (src/bindings.cpp:85;
+ * src/ct_projector_3d.cu:272-323, 403-433). */
+int ctlab_forward_project_3d_tvals(const float* volume, int64_t batch, int64_t n_x, int64_t n_y, int64_t n_z,
+                                   const float* tvals, int64_t n_int, const float* src, const float* dst,
+                                   int64_t n_ray, const float* M_inv, const float* b, float* out, void* stream);
+
+/* Replaces _C.back_project_3d_cuda (src/bindings.cpp:87;
+ * src/ct_projector_3d.cu:326-376, 435-462). */
+int ctlab_back_project_3d_tvals(const float* sino, int64_t batch, int64_t n_ray, const float* tvals,
+                                int64_t n_int, const float* src, const float* dst, const float* M_inv,
+                                const float* b, int64_t n_x, int64_t n_y, int64_t n_z, float* out, int accumulate,
+                                void* stream);
+
+/* Replaces _C.compress_tvals_3d_cuda (src/bindings.cpp:90;
+ * src/ct_projector_3d.cu:160-212, 464-489).  Writes t_uint16 [n_ray, n_int],
+ * t_start [n_ray] and t_scale [n_ray] exactly as the reference kernel does. */
+int ctlab_compress_tvals_3d(const float* tvals, int64_t n_ray, int64_t n_int, const float* src,
+                            const float* dst, float voxel_diag_len, uint16_t* t_uint16, float* t_start,
+                            float* t_scale, void* stream);
+
+/* The compressor with a choice of encoder.  The reference has two that
+ * disagree: CTLAB_COMPRESS_CUDA is compress_tvals_3d_kernel
+ * (src/ct_projector_3d.cu:160-212; what ctlab_compress_tvals_3d does);
+ * CTLAB_COMPRESS_TORCH is compress_tvals_to_uint16
+ * (tomography/ct_projector_3d_torch.py:4-65), which CTProjector3DModule uses
+ * for its own precompute (ct_projector_3d_module.py:100-102): +inf becomes
+ * 10.0, rounding is half to even and the running sum is a float. */
+#define CTLAB_COMPRESS_CUDA 0
+#define CTLAB_COMPRESS_TORCH 1
+int ctlab_compress_tvals_3d_ex(const float* tvals, int64_t n_ray, int64_t n_int, const float* src, const float* dst,
+                               float voxel_diag_len, uint16_t* t_uint16, float* t_start, float* t_scale, int mode,
+                               void* stream);
+
+/* Replaces _C.forward_project_3d_compressed_cuda (src/bindings.cpp:92;
+ * src/ct_projector_3d.cu:99-157, 491-522). */
+int ctlab_forward_project_3d_compressed(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
+                                        int64_t n_z, const uint16_t* t_uint16, const float* t_start,
+                                        const float* t_scale, int64_t n_int, const float* src, const float* dst,
+                                        int64_t n_ray, const float* M_inv, const float* b, float* out,
+                                        void* stream);
+
+/* Replaces _C.back_project_3d_compressed_cuda (src/bindings.cpp:94;
+ * src/ct_projector_3d.cu:215-269, 524-553). */
+int ctlab_back_project_3d_compressed(const float* sino, int64_t batch, int64_t n_ray, const uint16_t* t_uint16,
+                                     const float* t_start, const float* t_scale, int64_t n_int, const float* src,
+                                     const float* dst, const float* M_inv, const float* b, int64_t n_x,
+                                     int64_t n_y, int64_t n_z, float* out, int accumulate, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* 2-D                                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces _C.compute_intersections_2d (src/bindings.cpp:67;
+ * src/ct_projector_2d.cu:36-73, 158-177). n_int = (n_row+1)+(n_col+1). */
+int ctlab_compute_intersections_2d(int64_t n_row, int64_t n_col, const float* src, const float* dst,
+                                   int64_t n_ray, const float* M_inv, const float* b, float* t_out,
+                                   void* stream);
+
+/* Replaces _C.forward_project_2d_cuda (src/bindings.cpp:69;
+ * src/ct_projector_2d.cu:76-114, 179-200). */
+int ctlab_forward_project_2d_tvals(const float* image, int64_t batch, int64_t n_row, int64_t n_col,
+                                   const float* tvals, int64_t n_int, const float* src, const float* dst,
+                                   int64_t n_ray, const float* M_inv, const float* b, float* out, void* stream);
+
+/* Replaces _C.back_project_2d_cuda (src/bindings.cpp:71;
+ * src/ct_projector_2d.cu:117-155, 202-221). */
+int ctlab_back_project_2d_tvals(const float* sino, int64_t batch, int64_t n_ray, const float* tvals,
+                                int64_t n_int, const float* src, const float* dst, const float* M_inv,
+                                const float* b, int64_t n_row, int64_t n_col, float* out, int accumulate,
+                                void* stream);
+
+/* Replaces _C.forward_project_2d_on_the_fly_cuda (src/bindings.cpp:75;
+ * src/ct_projector_2d.cu:246-331, 416-440), keeping its incremental march
+ * (t_next += dt) so results follow that kernel rather than the tvals path. */
+int ctlab_forward_project_2d_on_the_fly(const float* image, int64_t batch, int64_t n_row, int64_t n_col,
+                                        const float* src, const float* dst, int64_t n_ray, const float* M_inv,
+                                        const float* b, float* out, void* stream);
+
+/* Replaces _C.back_project_2d_on_the_fly_cuda (src/bindings.cpp:78;
+ * src/ct_projector_2d.cu:334-413, 442-465). */
+int ctlab_back_project_2d_on_the_fly(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                     const float* dst, const float* M_inv, const float* b, int64_t n_row,
+                                     int64_t n_col, float* out, int accumulate, void* stream);
+
+/* 2-D Siddon without an intersection table, with the per-plane parameter
+ * arithmetic of the 3-D kernels (every plane parameter evaluated on its own,
+ * no drift).  Used by the 2-D module in place of the reference's
+ * precomputed-table path (ct_projector_2d_module.py:35-41, which stores
+ * [n_ray, n_int] tables), with the same results within float rounding. */
+int ctlab_forward_project_2d_siddon(const float* image, int64_t batch, int64_t n_row, int64_t n_col,
+                                    const float* src, const float* dst, int64_t n_ray, const float* M_inv,
+                                    const float* b, float* out, const ctlab_ray_tiling* tiling, void* stream);
+int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                 const float* dst, const float* M_inv, const float* b, int64_t n_row,
+                                 int64_t n_col, float* out, int accumulate, const ctlab_ray_tiling* tiling,
+                                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTLAB_B200_H */

@@ -1,0 +1,227 @@
+"""Parity of the CUDA kernels (called through the C ABI via the `_C` layer)
+with the CPU oracle, the reference's golden outputs and the adjoint identity.
+
+Tolerance (the projector's stated bar): 1e-5 relative, measured as
+max|ours - ref| / max|ref| over the output, in float32.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden, rel_err, rel_l2
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+DEV = "cuda"
+
+
+def T(a, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a)).to(DEV, dtype)
+
+
+def _c():
+    from ct_laboratory_b200 import _C
+    return _C
+
+
+def cone_case(n=(40, 36, 28), voxel=0.5, n_view=20, det=(48, 40), sid=120.0, sdd=180.0, pitch=0.6, seed=0):
+    from ct_laboratory_b200.tomography import build_conebeam_3d_geometry, standard_image_transform_3d
+    src, dst = build_conebeam_3d_geometry(n_view, det[0], det[1], sid, sdd, pitch)
+    M, b = standard_image_transform_3d(*n, voxel, voxel, voxel)
+    rng = np.random.default_rng(seed)
+    vol = rng.random(n).astype(np.float32)
+    return dict(dims=np.array(n), M=M.numpy(), Minv=O.minv(M.numpy()), b=b.numpy(), src=src.numpy(),
+                dst=dst.numpy(), vol=vol, y=rng.random(src.shape[0]).astype(np.float32), n_view=n_view, det=det)
+
+
+# --------------------------------------------------------------------------- 3-D on the fly
+@pytest.mark.parametrize("name", ["kat3d", "cone3d", "affine3d", "edge3d", "static3d"])
+def test_3d_on_the_fly_matches_oracle_and_golden(name):
+    C = _c()
+    g = load_golden(name)
+    d = [int(v) for v in g["dims"]]
+    Mi = T(g["Minv"])
+    fwd = C.forward_project_3d_on_the_fly_cuda(T(g["vol"]), T(g["src"]), T(g["dst"]), Mi, T(g["b"]))[0].cpu().numpy()
+    ref_ps = O.fwd_planesort(g["vol"], g["Minv"], g["b"], g["src"], g["dst"])
+    assert rel_err(fwd, ref_ps) < TOL
+    assert rel_err(fwd, g["fwd"]) < TOL
+    back = C.back_project_3d_on_the_fly_cuda(T(g["y"]), T(g["src"]), T(g["dst"]), Mi, T(g["b"]), *d)[0].cpu().numpy()
+    ref_b = O.back_planesort(g["y"], g["Minv"], g["b"], g["src"], g["dst"], d)
+    assert rel_err(back, ref_b) < TOL
+    assert rel_err(back, g["back"]) < TOL
+
+
+def test_3d_known_answer():
+    C = _c()
+    g = load_golden("kat3d")
+    out = C.forward_project_3d_on_the_fly_cuda(T(g["vol"]), T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"]))
+    assert abs(float(out[0, 0]) - 32.0) < 2e-5
+
+
+@pytest.mark.parametrize("tiled", [False, True])
+def test_3d_cone_medium_vs_oracle(tiled):
+    from ct_laboratory_b200 import _native as N
+    C = _c()
+    c = cone_case()
+    n_view, (nu, nv) = c["n_view"], c["det"]
+    til = N.tiling(n_view, nv, nu, nv * nu, nu, 1, tile_rows=32) if tiled else None
+    vol = np.stack([c["vol"], 1.0 - c["vol"]])  # batch of 2
+    out = C.forward_project_3d_on_the_fly_cuda(T(vol), T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]),
+                                               tiling=til).cpu().numpy()
+    for k in range(2):
+        ref = O.fwd_planesort(vol[k], c["Minv"], c["b"], c["src"], c["dst"])
+        assert rel_err(out[k], ref) < TOL and rel_l2(out[k], ref) < 1e-6
+    y = np.stack([c["y"], 2.0 * c["y"]])
+    back = C.back_project_3d_on_the_fly_cuda(T(y), T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]),
+                                             *[int(v) for v in c["dims"]], tiling=til).cpu().numpy()
+    ref = O.back_planesort(c["y"], c["Minv"], c["b"], c["src"], c["dst"], c["dims"])
+    assert rel_err(back[0], ref) < TOL
+    assert rel_err(back[1], 2.0 * ref) < TOL
+
+
+def test_3d_adjoint_identity():
+    """<A x, y> = <x, A^T y> (float64 accumulation of the float32 outputs)."""
+    C = _c()
+    c = cone_case(seed=3)
+    ax = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]))
+    aty = C.back_project_3d_on_the_fly_cuda(T(c["y"]), T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]),
+                                            *[int(v) for v in c["dims"]])
+    lhs = float(ax.double().flatten() @ T(c["y"]).double())
+    rhs = float((T(c["vol"]).double() * aty.double()[0]).sum())
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+
+
+def test_3d_fp64_oracle_bound():
+    """float32 kernel vs the FP64 oracle: error stays at float32 rounding."""
+    C = _c()
+    c = cone_case(n=(24, 24, 20), n_view=8, det=(32, 24), seed=5)
+    out = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(c["src"]), T(c["dst"]), T(c["Minv"]),
+                                               T(c["b"]))[0].cpu().numpy()
+    Mi64 = np.linalg.inv(c["M"].astype(np.float64))
+    ref64 = O.fwd_otf_torch(c["vol"], Mi64, c["b"], c["src"], c["dst"], dtype=np.float64)
+    assert rel_err(out, ref64) < 1e-5
+
+
+def test_3d_empty_and_missing_rays():
+    C = _c()
+    c = cone_case(n=(8, 8, 8), n_view=2, det=(8, 8))
+    src = np.zeros((0, 3), np.float32)
+    out = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(src), T(src), T(c["Minv"]), T(c["b"]))
+    assert out.shape == (1, 0)
+    back = C.back_project_3d_on_the_fly_cuda(T(np.zeros(0, np.float32)), T(src), T(src), T(c["Minv"]), T(c["b"]),
+                                             8, 8, 8)
+    assert back.shape == (1, 8, 8, 8) and float(back.abs().sum()) == 0.0
+    far = np.array([[1000.0, 1000.0, 0.0]], np.float32)
+    out = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(far), T(far + 1), T(c["Minv"]), T(c["b"]))
+    assert float(out[0, 0]) == 0.0
+
+
+def test_3d_errors_are_loud():
+    C = _c()
+    c = cone_case(n=(8, 8, 8), n_view=1, det=(4, 4))
+    with pytest.raises(RuntimeError):
+        C.forward_project_3d_on_the_fly_cuda(torch.zeros(8, 8, 8), T(c["src"]), T(c["dst"]), T(c["Minv"]),
+                                             T(c["b"]))
+    with pytest.raises(RuntimeError):
+        C.forward_project_3d_on_the_fly_cuda(T(c["vol"]).double(), T(c["src"]), T(c["dst"]), T(c["Minv"]),
+                                             T(c["b"]))
+    with pytest.raises(RuntimeError):
+        C.forward_project_3d_on_the_fly_cuda(T(c["vol"])[None, None], T(c["src"]), T(c["dst"]), T(c["Minv"]),
+                                             T(c["b"]))
+
+
+# --------------------------------------------------------------------------- 2-D
+@pytest.mark.parametrize("name", ["kat2d", "fan2d", "static2d"])
+def test_2d_siddon_matches_golden(name):
+    from ct_laboratory_b200.tomography import back_project_2d_siddon, forward_project_2d_siddon
+    g = load_golden(name)
+    Mi = T(g["Minv"])
+    fwd = forward_project_2d_siddon(T(g["img"]), Mi, T(g["b"]), T(g["src"]), T(g["dst"]))[0].cpu().numpy()
+    assert rel_err(fwd, g["fwd"]) < TOL
+    back = back_project_2d_siddon(T(g["y"]), Mi, T(g["b"]), T(g["src"]), T(g["dst"]),
+                                  *[int(v) for v in g["dims"]])[0].cpu().numpy()
+    assert rel_err(back, g["back"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["kat2d", "fan2d", "static2d"])
+def test_2d_reference_march_matches_oracle(name):
+    C = _c()
+    g = load_golden(name)
+    d = [int(v) for v in g["dims"]]
+    fwd = C.forward_project_2d_on_the_fly_cuda(T(g["img"]), T(g["src"]), T(g["dst"]), T(g["Minv"]),
+                                               T(g["b"]))[0].cpu().numpy()
+    assert rel_err(fwd, O.fwd_dda2(g["img"], g["Minv"], g["b"], g["src"], g["dst"])) < TOL
+    back = C.back_project_2d_on_the_fly_cuda(T(g["y"]), T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"]),
+                                             *d)[0].cpu().numpy()
+    assert rel_err(back, O.back_dda2(g["y"], g["Minv"], g["b"], g["src"], g["dst"], d)) < TOL
+
+
+@pytest.mark.parametrize("name", ["kat2d", "fan2d", "static2d"])
+def test_2d_tables(name):
+    C = _c()
+    g = load_golden(name)
+    d = [int(v) for v in g["dims"]]
+    tv = C.compute_intersections_2d(*d, T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"])).cpu().numpy()
+    assert np.array_equal(tv, g["tvals"])
+    fwd = C.forward_project_2d_cuda(T(g["img"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]),
+                                    T(g["b"]))[0].cpu().numpy()
+    assert rel_err(fwd, g["fwd"]) < TOL
+    back = C.back_project_2d_cuda(T(g["y"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"]),
+                                  *d)[0].cpu().numpy()
+    assert rel_err(back, g["back"]) < TOL
+
+
+# --------------------------------------------------------------------------- 3-D tables
+@pytest.mark.parametrize("name", ["kat3d", "cone3d", "affine3d", "edge3d", "static3d"])
+def test_3d_tables(name):
+    C = _c()
+    g = load_golden(name)
+    d = [int(v) for v in g["dims"]]
+    tv = C.compute_intersections_3d(*d, T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"])).cpu().numpy()
+    if name == "affine3d":
+        fin = np.isfinite(g["tvals"])
+        assert np.array_equal(fin, np.isfinite(tv)) and np.abs(tv[fin] - g["tvals"][fin]).max() < 1e-5
+    else:
+        assert np.array_equal(tv, g["tvals"])
+    fwd = C.forward_project_3d_cuda(T(g["vol"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]),
+                                    T(g["b"]))[0].cpu().numpy()
+    assert rel_err(fwd, g["fwd"]) < TOL
+    back = C.back_project_3d_cuda(T(g["y"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"]),
+                                  *d)[0].cpu().numpy()
+    assert rel_err(back, g["back"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["cone3d", "affine3d"])
+def test_compressed_codec_and_projector(name):
+    C = _c()
+    g = load_golden(name)
+    d = [int(v) for v in g["dims"]]
+    # torch encoder: bit-exact with the reference's compress_tvals_to_uint16
+    t16, st, sc = C.compress_tvals_3d_mode(T(g["tvals"]), T(g["src"]), T(g["dst"]), float(g["voxel_diag"]), mode=1)
+    assert np.array_equal(t16.cpu().numpy().view(np.uint16), g["u16"])
+    assert np.array_equal(st.cpu().numpy(), g["starts"]) and np.array_equal(sc.cpu().numpy(), g["scales"])
+    # CUDA encoder: bit-exact with the restated reference kernel
+    t16c, stc, scc = C.compress_tvals_3d_cuda(T(g["tvals"]), T(g["src"]), T(g["dst"]), float(g["voxel_diag"]))
+    u_o, st_o, sc_o = O.compress_cuda(g["tvals"], g["src"], g["dst"], float(g["voxel_diag"]))
+    assert np.array_equal(scc.cpu().numpy(), sc_o) and np.array_equal(stc.cpu().numpy(), st_o)
+    assert np.array_equal(t16c.cpu().numpy().view(np.uint16), u_o)
+    # decode + project, both encoders' streams
+    for (u, s_, c_) in ((g["u16"], g["starts"], g["scales"]), (u_o, st_o, sc_o)):
+        ut = T(u.view(np.int16), torch.int16)
+        fwd = C.forward_project_3d_compressed_cuda(T(g["vol"]), ut, T(s_), T(c_), T(g["src"]), T(g["dst"]),
+                                                   T(g["Minv"]), T(g["b"]))[0].cpu().numpy()
+        assert rel_err(fwd, O.fwd_comp_cuda(g["vol"], u, s_, c_, g["Minv"], g["b"], g["src"], g["dst"])) < TOL
+        back = C.back_project_3d_compressed_cuda(T(g["y"]), ut, T(s_), T(c_), T(g["src"]), T(g["dst"]),
+                                                 T(g["Minv"]), T(g["b"]), *d)[0].cpu().numpy()
+        assert rel_err(back, O.back_comp_cuda(g["y"], u, s_, c_, g["Minv"], g["b"], g["src"], g["dst"], d)) < TOL
+
+
+def test_invert_matrix_exact_for_diagonal():
+    from ct_laboratory_b200.tomography._common import inverse
+    for s in (0.5, 0.7, 0.8, 1.0, 1.5, 3.2):
+        M = torch.diag(torch.tensor([s, s * 1.1, s * 0.9], dtype=torch.float32))
+        got = inverse(M.to(DEV)).cpu()
+        assert torch.equal(got, torch.inverse(M))
+    R = torch.tensor([[0.8, -0.2, 0.1], [0.3, 1.1, 0.0], [0.05, 0.0, 0.6]])
+    assert torch.allclose(inverse(R.to(DEV)).cpu(), torch.inverse(R), rtol=1e-6, atol=1e-6)
