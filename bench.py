@@ -47,7 +47,7 @@ sys.path.insert(0, ROOT)
 # frozen from the FP64 oracle: `python oracle/count_segments.py <workload>`.
 SEGMENTS = {
     "fan256": 45_364_441,
-    "cone256": None,  # filled below once counted
+    "cone256": 6_962_229_058,
 }
 METRIC = "GRays/s fwd+adj"
 L2_FLUSH_BYTES = 512 << 20
@@ -249,7 +249,9 @@ def run_ours(args, world, rank, local):
     dev = torch.device("cuda", local)
     if w.name.startswith("cone"):
         proj = ConeBeam3DProjector(*w.n, n_view=w.n_view, det_nx=w.det_nx, det_ny=w.det_ny, sid=w.sid, sdd=w.sdd,
-                                   det_spacing=w.pitch, voxel_size=w.voxel, device=dev, tile_rows=args.tile_rows)
+                                   det_spacing=w.pitch, voxel_size=w.voxel, device=dev, tile_rows=args.tile_rows,
+                                   voxel_rule=args.voxel_rule, walk=args.walk,
+                                   deterministic_adjoint=args.deterministic)
     else:
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
                                   pixel_size=w.pixel, device=dev)
@@ -314,7 +316,10 @@ def run_ours(args, world, rank, local):
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": {"workload": w.name, "n_ray": n_ray, "volume": list(w.n),
                           "views": w.n_view, "rays_per_rank": n_ray, "l2": "flushed (512 MiB write) before each step",
-                          "tile_rows": args.tile_rows, "parallelism": f"independent scans x{world}"},
+                          "tile_rows": args.tile_rows, "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
+                          "walk": ["auto", "lane", "column"][args.walk],
+                          "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
+                          "parallelism": f"independent scans x{world}"},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(out))
@@ -378,6 +383,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="cone256")
     ap.add_argument("--tile-rows", type=int, default=32)
+    ap.add_argument("--voxel-rule", type=int, default=1, help="0 = reference midpoint rule, 1 = crossing rule")
+    ap.add_argument("--walk", type=int, default=0, help="0 = auto, 1 = per-lane walk, 2 = column walk")
+    ap.add_argument("--deterministic", action="store_true", help="adjoint by the voxel-driven gather")
     ap.add_argument("--views", type=int, default=0,
                     help="override the workload's view count (smaller cases for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=5)

@@ -26,15 +26,20 @@ _I = ctypes.c_int
 _F = ctypes.c_float
 
 
-class RayTiling(ctypes.Structure):
-    """Mirror of ctlab_ray_tiling (include/ctlab_b200.h)."""
+VOXEL_MIDPOINT = 0  # the reference's rule: rounded world-space segment midpoint
+VOXEL_CROSSING = 1  # the voxel enclosed by the two bounding crossings (exact topology)
+WALK_AUTO, WALK_LANE, WALK_COLUMN = 0, 1, 2
+
+
+class RayOpts(ctypes.Structure):
+    """Mirror of ctlab_ray_opts (include/ctlab_b200.h): ray tiling + voxel rule."""
 
     _fields_ = [("n_view", _I64), ("n_row", _I64), ("n_col", _I64), ("view_stride", _I64),
                 ("row_stride", _I64), ("col_stride", _I64), ("tile_rows", ctypes.c_int32),
-                ("block_threads", ctypes.c_int32)]
+                ("block_threads", ctypes.c_int32), ("voxel_rule", ctypes.c_int32), ("walk", ctypes.c_int32)]
 
 
-_TP = ctypes.POINTER(RayTiling)
+_TP = ctypes.POINTER(RayOpts)
 
 # name -> argtypes (every entry point returns int)
 _SIGS = {
@@ -59,6 +64,7 @@ _SIGS = {
     "ctlab_forward_project_2d_siddon": [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _TP, _P],
     "ctlab_back_project_2d_siddon": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P],
     "ctlab_invert_matrix": [_P, _I, _P, _P, _P],
+    "ctlab_back_project_3d_gather": [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I64, _P, _P],
 }
 
 for _name, _args in _SIGS.items():
@@ -97,9 +103,16 @@ def stream_of(t: torch.Tensor):
     return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
 
 
-def tiling(n_view, n_row, n_col, view_stride, row_stride, col_stride, tile_rows=32, block_threads=256):
-    return RayTiling(int(n_view), int(n_row), int(n_col), int(view_stride), int(row_stride), int(col_stride),
-                     int(tile_rows), int(block_threads))
+def tiling(n_view, n_row, n_col, view_stride, row_stride, col_stride, tile_rows=32, block_threads=256,
+           voxel_rule=VOXEL_MIDPOINT, walk=WALK_AUTO):
+    """Launch options for rays laid out as a [view][row][col] grid."""
+    return RayOpts(int(n_view), int(n_row), int(n_col), int(view_stride), int(row_stride), int(col_stride),
+                   int(tile_rows), int(block_threads), int(voxel_rule), int(walk))
+
+
+def flat_opts(voxel_rule=VOXEL_MIDPOINT, block_threads=256):
+    """Launch options for a flat ray list with a chosen voxel rule."""
+    return RayOpts(0, 0, 0, 0, 0, 0, 0, int(block_threads), int(voxel_rule), WALK_AUTO)
 
 
 def tiling_ref(t):

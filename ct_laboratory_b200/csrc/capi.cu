@@ -16,23 +16,31 @@ int set_error(int code, const char* fmt, ...) {
 
 void clear_error() { g_last_error[0] = '\0'; }
 
-int resolve_tiling(const ctlab_ray_tiling* t, int64_t n_ray, Tiling& T) {
-    if (t == nullptr) {
+int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& T) {
+    const bool flat = t == nullptr || (t->n_view == 0 && t->n_row == 0 && t->n_col == 0);
+    int threads = 256, rows = 256;
+    if (t != nullptr) {
+        CTLAB_REQUIRE(t->voxel_rule == CTLAB_VOXEL_MIDPOINT || t->voxel_rule == CTLAB_VOXEL_CROSSING,
+                      "ray options: unknown voxel_rule %d", t->voxel_rule);
+        CTLAB_REQUIRE(t->walk == CTLAB_WALK_AUTO || t->walk == CTLAB_WALK_LANE || t->walk == CTLAB_WALK_COLUMN,
+                      "ray options: unknown walk %d", t->walk);
+        threads = t->block_threads ? t->block_threads : 256;
+        rows = t->tile_rows ? t->tile_rows : (flat ? threads : 32);
+        CTLAB_REQUIRE(threads >= 32 && threads <= 256 && threads % 32 == 0,
+                      "ray tiling: block_threads must be a multiple of 32 in [32, 256] (got %d)", threads);
+        CTLAB_REQUIRE(rows >= 1 && rows <= threads && threads % rows == 0,
+                      "ray tiling: tile_rows must divide block_threads (got %d, %d)", rows, threads);
+    }
+    if (flat) {
         T.n_view = 1;
         T.n_row = n_ray;
         T.n_col = 1;
         T.view_stride = n_ray;
         T.row_stride = 1;
         T.col_stride = 1;
-        T.tile_rows = 256;
+        T.tile_rows = threads;
         T.tile_cols = 1;
     } else {
-        const int threads = t->block_threads ? t->block_threads : 256;
-        const int rows = t->tile_rows ? t->tile_rows : 32;
-        CTLAB_REQUIRE(threads >= 32 && threads <= 1024 && threads % 32 == 0,
-                      "ray tiling: block_threads must be a multiple of 32 in [32, 1024] (got %d)", threads);
-        CTLAB_REQUIRE(rows >= 1 && rows <= threads && threads % rows == 0,
-                      "ray tiling: tile_rows must divide block_threads (got %d, %d)", rows, threads);
         CTLAB_REQUIRE(t->n_view >= 1 && t->n_row >= 1 && t->n_col >= 1, "ray tiling: empty grid");
         CTLAB_REQUIRE(t->n_view * t->n_row * t->n_col == n_ray,
                       "ray tiling: n_view*n_row*n_col (%lld) must equal n_ray (%lld)",

@@ -129,7 +129,7 @@ struct Tiling {
 };
 
 // Validates `t` (may be NULL = flat) against n_ray and fills `out`.
-int resolve_tiling(const ctlab_ray_tiling* t, int64_t n_ray, Tiling& out);
+int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& out);
 
 // Ray handled by this thread, or -1 when the thread's slot is outside the grid.
 __device__ __forceinline__ int64_t tile_ray(const Tiling& T) {

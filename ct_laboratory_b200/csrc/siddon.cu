@@ -38,9 +38,34 @@ struct GridDims {
     int stride[NDIM];
 };
 
+// Voxel of a segment [t0, t1] under the reference's rule: the world-space
+// midpoint s + t_mid*v mapped to index space and rounded half to even
+// (ct_projector_3d.cu:982-996).  Returns the flat index or -1 (outside).
+template <int NDIM>
+__device__ __forceinline__ int midpoint_voxel(const AffineT<NDIM>& A, const float* sw, const float* vw, float t0,
+                                              float t1, const GridDims<NDIM>& G) {
+    const float tm = __fmul_rn(0.5f, __fadd_rn(t0, t1));
+    float m[NDIM], f[NDIM];
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) m[a] = __fmaf_rn(tm, vw[a], sw[a]);
+    if constexpr (NDIM == 3) world_to_index3(A, m[0], m[1], m[2], f[0], f[1], f[2]);
+    else world_to_index2(A, m[0], m[1], f[0], f[1]);
+    int flat = 0;
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        const int i = __float2int_rn(f[a]);
+        ok = ok && i >= 0 && i < G.n[a];
+        flat += i * G.stride[a];
+    }
+    return ok ? flat : -1;
+}
+
 // One Siddon traversal.  ADJ=false: returns sum of in[voxel]*len.
-// ADJ=true: scatters y*len into out[voxel].
-template <int NDIM, bool ADJ>
+// ADJ=true: scatters y*len into out[voxel].  MID selects the voxel of each
+// segment: true = the reference's rounded world midpoint, false = the voxel
+// between the two crossings that bound the segment (exact topology).
+template <int NDIM, bool ADJ, bool MID>
 __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* __restrict__ out, float y,
                                           const float* sw, const float* dw, const GridDims<NDIM>& G,
                                           const AffineT<NDIM>& A, unsigned nvox) {
@@ -133,6 +158,58 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
     for (int a = 0; a < NDIM; ++a) max_it += G.n[a];
     float acc = 0.f;
     float t_cur = t_enter;
+    if constexpr (!ADJ && !MID) {
+        // Forward, crossing rule: walk four segments, then issue their four
+        // gathers back to back and accumulate them in walk order (the sum is
+        // the same sequence of fused multiply-adds as one at a time, so the
+        // result is bitwise that of the loop below).  Four loads in flight
+        // per lane instead of one hides the L2 latency of the gathers.
+        bool done = false;
+#pragma unroll 1
+        for (int it = 0; it < max_it && !done; it += 4) {
+            int vq[4];
+            float sq[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vq[q] = 0;
+                sq[q] = 0.f;
+                if (done) continue;
+                float tm = tn[0];
+#pragma unroll
+                for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
+                const bool fin = !(tm < t_exit);
+                const float t1 = fin ? t_exit : tm;
+                if (t1 > t_cur && (unsigned)idx < nvox) {
+                    vq[q] = idx;
+                    sq[q] = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                }
+                done = fin;
+                if (!fin) {
+                    t_cur = t1;
+                    if (tn[0] == tm) {
+                        idx += ds[0];
+                        pn[0] += ps[0];
+                        tn[0] = plane_t(pn[0], s[0], inv[0]);
+                    } else if (NDIM == 2 || tn[1] == tm) {
+                        idx += ds[1];
+                        pn[1] += ps[1];
+                        tn[1] = plane_t(pn[1], s[1], inv[1]);
+                    } else {
+                        idx += ds[NDIM - 1];
+                        pn[NDIM - 1] += ps[NDIM - 1];
+                        tn[NDIM - 1] = plane_t(pn[NDIM - 1], s[NDIM - 1], inv[NDIM - 1]);
+                    }
+                }
+            }
+            float vv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) vv[q] = sq[q] != 0.f ? __ldg(vol + vq[q]) : 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (sq[q] != 0.f) acc = __fmaf_rn(vv[q], sq[q], acc);
+        }
+        return acc;
+    }
 #pragma unroll 1
     for (int it = 0; it < max_it; ++it) {
         float tm = tn[0];
@@ -140,13 +217,16 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
         for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
         const bool fin = !(tm < t_exit);
         const float t1 = fin ? t_exit : tm;
-        if (t1 > t_cur && (unsigned)idx < nvox) {
-            // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
-            const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
-            if constexpr (ADJ) {
-                atomicAdd(out + idx, __fmul_rn(y, seg));
-            } else {
-                acc = __fmaf_rn(__ldg(vol + idx), seg, acc);
+        if (t1 > t_cur) {
+            const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
+            if ((unsigned)v < nvox) {
+                // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
+                const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                if constexpr (ADJ) {
+                    atomicAdd(out + v, __fmul_rn(y, seg));
+                } else {
+                    acc = __fmaf_rn(__ldg(vol + v), seg, acc);
+                }
             }
         }
         if (fin) break;
@@ -170,7 +250,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
     return acc;
 }
 
-template <int NDIM, bool ADJ>
+template <int NDIM, bool ADJ, bool MID>
 __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                      const float* __restrict__ src, const float* __restrict__ dst,
                                                      int64_t n_ray, const float* __restrict__ M_inv,
@@ -194,9 +274,269 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
     if constexpr (ADJ) {
         const float y = __ldg(in + bi * n_ray + r);
         if (y == 0.f) return;  // contributes exactly nothing
-        traverse<NDIM, true>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
+        traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
     } else {
-        out[bi * n_ray + r] = traverse<NDIM, false>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox);
+        out[bi * n_ray + r] =
+            traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Column-coherent 3-D traversal.
+//
+// When the 32 lanes of a warp trace rays that share their x-y line (same
+// source, same detector column of a detector whose columns run along z: the
+// cone-beam and StaticCT rings), every x- and y-plane parameter is bitwise
+// the same for all lanes; only the z planes differ.  The per-lane merge walk
+// above then diverges at almost every step (some lane always takes a z step)
+// and the lanes drift apart along the x-y path.  Here the warp walks the x-y
+// cells together (warp-uniform state) and each lane splits a cell only at its
+// own z planes.  The segment end points are the same floats and they are
+// accumulated in the same order as in traverse(), so results are bitwise those
+// of the general walk; the gathers (forward) and reductions (adjoint) of a
+// warp now address one voxel column (i, j, k..k+~32) at a time.
+// A warp whose lanes do not share the x-y line falls back to traverse().
+// ----------------------------------------------------------------------------
+constexpr unsigned kFullMask = 0xffffffffu;
+
+struct LaneRay {
+    float s[3], inv[3], ray_len, t_enter, t_exit;
+    bool live;
+};
+
+// Per-lane set-up, identical arithmetic to the start of traverse<3>.
+__device__ __forceinline__ void lane_setup(LaneRay& R, const float* sw, const float* dw, const GridDims<3>& G,
+                                           const Affine3& A, int& fixed_idx, bool& z_parallel) {
+    float vw[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
+    R.ray_len = sqrtf(sumsq3(vw[0], vw[1], vw[2]));
+    R.live = R.ray_len >= 1e-12f;
+    float d[3];
+    world_to_index3(A, sw[0], sw[1], sw[2], R.s[0], R.s[1], R.s[2]);
+    world_to_index3(A, dw[0], dw[1], dw[2], d[0], d[1], d[2]);
+    R.t_enter = 0.f;
+    R.t_exit = 1.f;
+    fixed_idx = 0;
+    z_parallel = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float va = __fsub_rn(d[a], R.s[a]);
+        const float nf = (float)G.n[a];
+        R.live = R.live && isfinite(R.s[a]) && isfinite(va);
+        if (fabsf(va) > 1e-12f) {
+            R.inv[a] = __frcp_rn(va);
+            const float lo = va > 0.f ? -0.5f : nf - 0.5f;
+            const float hi = va > 0.f ? nf - 0.5f : -0.5f;
+            R.t_enter = fmaxf(R.t_enter, plane_t(lo, R.s[a], R.inv[a]));
+            R.t_exit = fminf(R.t_exit, plane_t(hi, R.s[a], R.inv[a]));
+        } else {
+            R.inv[a] = 0.f;
+            const int i = __float2int_rn(R.s[a]);
+            R.live = R.live && (i >= 0) && (i < G.n[a]);
+            fixed_idx += i * G.stride[a];
+            if (a == 2) z_parallel = true;
+        }
+    }
+    R.live = R.live && (R.t_enter < R.t_exit);
+}
+
+// Slab index of a crossing axis at time t: behind-plane parameter <= t and
+// ahead-plane parameter > t (the fix-up of traverse), clamped into the grid.
+__device__ __forceinline__ int slab_at(float t, float s, float inv, int n) {
+    const float va_sign = inv;  // same sign as v
+    const float c = __fmaf_rn(t, __frcp_rn(inv), s);
+    int i = __float2int_rd(c + 0.5f);
+    if (va_sign > 0.f) {
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s, inv) <= t; ++k) ++i;
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s, inv) > t; ++k) --i;
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s, inv) <= t; ++k) --i;
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s, inv) > t; ++k) ++i;
+    }
+    return min(max(i, 0), n - 1);
+}
+
+template <bool ADJ, bool MID>
+__global__ void __launch_bounds__(256) siddon3d_column_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                              const float* __restrict__ src,
+                                                              const float* __restrict__ dst, int64_t n_ray,
+                                                              const float* __restrict__ M_inv,
+                                                              const float* __restrict__ bvec, GridDims<3> G,
+                                                              int64_t nvox, Tiling T) {
+    const int64_t r = tile_ray(T);
+    const int64_t bi = blockIdx.y;
+    const Affine3 A = load_affine3(M_inv, bvec);
+    float sw[3] = {0.f, 0.f, 0.f}, dw[3] = {0.f, 0.f, 0.f};
+    if (r >= 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            sw[a] = __ldg(src + r * 3 + a);
+            dw[a] = __ldg(dst + r * 3 + a);
+        }
+    }
+    float y = 0.f;
+    if constexpr (ADJ) {
+        if (r >= 0) y = __ldg(in + bi * n_ray + r);
+    }
+    LaneRay R;
+    int fixed_idx;
+    bool z_par;
+    lane_setup(R, sw, dw, G, A, fixed_idx, z_par);
+    R.live = R.live && (r >= 0) && (!ADJ || y != 0.f);
+
+    // Do the live lanes share their x-y line?  (Inactive lanes do not vote.)
+    const unsigned live_mask = __ballot_sync(kFullMask, R.live);
+    if (live_mask == 0u) {
+        if (!ADJ && r >= 0) out[bi * n_ray + r] = 0.f;
+        return;
+    }
+    const int leader = __ffs(live_mask) - 1;
+    const float s0 = __shfl_sync(kFullMask, R.s[0], leader), s1 = __shfl_sync(kFullMask, R.s[1], leader);
+    const float i0 = __shfl_sync(kFullMask, R.inv[0], leader), i1 = __shfl_sync(kFullMask, R.inv[1], leader);
+    const bool same = !R.live || (__float_as_uint(R.s[0]) == __float_as_uint(s0) &&
+                                  __float_as_uint(R.s[1]) == __float_as_uint(s1) &&
+                                  __float_as_uint(R.inv[0]) == __float_as_uint(i0) &&
+                                  __float_as_uint(R.inv[1]) == __float_as_uint(i1));
+    if (!__all_sync(kFullMask, same)) {
+        // lanes do not share the x-y line: per-lane merge walk
+        if (r < 0) return;
+        if constexpr (ADJ) {
+            if (R.live) traverse<3, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
+        } else {
+            out[bi * n_ray + r] =
+                R.live ? traverse<3, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox) : 0.f;
+        }
+        return;
+    }
+
+    // ---- warp-uniform x-y walk (every lane holds the same values) ----------
+    const float nx = (float)G.n[0], ny = (float)G.n[1];
+    float txy_in = 0.f, txy_out = 1.f;
+    bool xy_ok = true;
+    int col = 0;  // flat index of the current (i, j) column, k = 0
+    float tnx = __int_as_float(0x7f800000), tny = tnx, pnx = 0.f, pny = 0.f, psx = 0.f, psy = 0.f;
+    int dsx = 0, dsy = 0;
+    if (i0 != 0.f) {
+        const bool pos = i0 > 0.f;
+        txy_in = fmaxf(txy_in, plane_t(pos ? -0.5f : nx - 0.5f, s0, i0));
+        txy_out = fminf(txy_out, plane_t(pos ? nx - 0.5f : -0.5f, s0, i0));
+    } else {
+        const int i = __float2int_rn(s0);
+        xy_ok = xy_ok && i >= 0 && i < G.n[0];
+        col += i * G.stride[0];
+    }
+    if (i1 != 0.f) {
+        const bool pos = i1 > 0.f;
+        txy_in = fmaxf(txy_in, plane_t(pos ? -0.5f : ny - 0.5f, s1, i1));
+        txy_out = fminf(txy_out, plane_t(pos ? ny - 0.5f : -0.5f, s1, i1));
+    } else {
+        const int j = __float2int_rn(s1);
+        xy_ok = xy_ok && j >= 0 && j < G.n[1];
+        col += j * G.stride[1];
+    }
+    // Every live lane's own interval [t_enter, t_exit] lies inside
+    // [txy_in, txy_out]; walk only the union of the lanes' intervals.
+    float te = R.live ? R.t_enter : __int_as_float(0x7f800000);
+    float tx = R.live ? R.t_exit : __int_as_float(0xff800000);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        te = fminf(te, __shfl_xor_sync(kFullMask, te, o));
+        tx = fmaxf(tx, __shfl_xor_sync(kFullMask, tx, o));
+    }
+    txy_in = fmaxf(txy_in, te);
+    txy_out = fminf(txy_out, tx);
+    xy_ok = xy_ok && txy_in < txy_out;
+    if (i0 != 0.f) {
+        const int i = slab_at(txy_in, s0, i0, G.n[0]);
+        col += i * G.stride[0];
+        psx = i0 > 0.f ? 1.f : -1.f;
+        dsx = i0 > 0.f ? G.stride[0] : -G.stride[0];
+        pnx = (float)i + 0.5f * psx;
+        tnx = plane_t(pnx, s0, i0);
+    }
+    if (i1 != 0.f) {
+        const int j = slab_at(txy_in, s1, i1, G.n[1]);
+        col += j * G.stride[1];
+        psy = i1 > 0.f ? 1.f : -1.f;
+        dsy = i1 > 0.f ? G.stride[1] : -G.stride[1];
+        pny = (float)j + 0.5f * psy;
+        tny = plane_t(pny, s1, i1);
+    }
+
+    // ---- per-lane z state, started at the lane's own entry ----------------
+    float tnz = __int_as_float(0x7f800000), pnz = 0.f, psz = 0.f;
+    int kz = 0, dsz = 0;
+    if (R.live) {
+        if (!z_par) {
+            const int k = slab_at(R.t_enter, R.s[2], R.inv[2], G.n[2]);
+            kz = k * G.stride[2];
+            psz = R.inv[2] > 0.f ? 1.f : -1.f;
+            dsz = R.inv[2] > 0.f ? G.stride[2] : -G.stride[2];
+            pnz = (float)k + 0.5f * psz;
+            tnz = plane_t(pnz, R.s[2], R.inv[2]);
+        } else {
+            kz = fixed_idx - (fixed_idx / G.stride[1]) * G.stride[1];  // the k part of the fixed index
+        }
+    }
+    const float* vol = in + bi * nvox;
+    float* vout = out + bi * nvox;
+    float acc = 0.f;
+    const int max_xy = G.n[0] + G.n[1] + 3;
+    const int max_z = G.n[2] + 3;
+    int zsteps = 0;
+    float ta = txy_in;
+#pragma unroll 1
+    for (int it = 0; it < max_xy && xy_ok; ++it) {
+        const float tm = fminf(tnx, tny);
+        const bool last = !(tm < txy_out);
+        const float tb = last ? txy_out : tm;
+        if (R.live) {
+            float t0 = fmaxf(ta, R.t_enter);
+            const float tend = fminf(tb, R.t_exit);
+#pragma unroll 1
+            while (t0 < tend && zsteps < max_z) {
+                if (tnz <= t0) {  // a z plane at or before t0 has been crossed
+                    kz += dsz;
+                    pnz += psz;
+                    tnz = plane_t(pnz, R.s[2], R.inv[2]);
+                    ++zsteps;
+                    continue;
+                }
+                const float t1 = fminf(tend, tnz);
+                int idx = col + kz;
+                if constexpr (MID) {
+                    float vw[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
+                    idx = midpoint_voxel<3>(A, sw, vw, t0, t1, G);
+                }
+                if ((unsigned)idx < (unsigned)nvox) {
+                    const float seg = __fmul_rn(__fsub_rn(t1, t0), R.ray_len);
+                    if constexpr (ADJ) atomicAdd(vout + idx, __fmul_rn(y, seg));
+                    else acc = __fmaf_rn(__ldg(vol + idx), seg, acc);
+                }
+                t0 = t1;
+            }
+        }
+        if (last) break;
+        ta = tb;
+        if (tnx == tm) {
+            col += dsx;
+            pnx += psx;
+            tnx = plane_t(pnx, s0, i0);
+        } else {
+            col += dsy;
+            pny += psy;
+            tny = plane_t(pny, s1, i1);
+        }
+    }
+    if constexpr (!ADJ) {
+        if (r >= 0) out[bi * n_ray + r] = acc;
     }
 }
 
@@ -207,7 +547,7 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
 template <int NDIM, bool ADJ>
 static int launch_siddon(const char* what, const float* in, float* out, int64_t batch, const int64_t* dims,
                          const float* src, const float* dst, int64_t n_ray, const float* M_inv, const float* b,
-                         int accumulate, const ctlab_ray_tiling* tiling, void* stream) {
+                         int accumulate, const ctlab_ray_opts* tiling, void* stream) {
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535], got %lld", what, (long long)batch);
     CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
     GridDims<NDIM> G;
@@ -224,8 +564,12 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
         G.stride[a] = (int)st;
         st *= dims[a];
     }
-    CTLAB_REQUIRE(in && out && M_inv && b, "%s: null data pointer", what);
-    CTLAB_REQUIRE(n_ray == 0 || (src && dst), "%s: null src/dst", what);
+    // Buffers of zero elements may be NULL (torch gives empty tensors a null
+    // data pointer); the volume side is never empty.
+    const bool vol_ok = ADJ ? (out != nullptr) : (in != nullptr);
+    const bool ray_ok = n_ray == 0 || (src && dst && (ADJ ? in != nullptr : out != nullptr));
+    CTLAB_REQUIRE(vol_ok && M_inv && b, "%s: null data pointer", what);
+    CTLAB_REQUIRE(ray_ok, "%s: null src/dst/sinogram", what);
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) {
         CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
@@ -234,11 +578,30 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     Tiling T;
     int rc = resolve_tiling(tiling, n_ray, T);
     if (rc) return rc;
-    CTLAB_REQUIRE(T.tile_rows * T.tile_cols <= 256, "%s: block_threads must be <= 256", what);
     CTLAB_REQUIRE(T.n_blocks <= kMaxGrid, "%s: too many rays for one launch", what);
     dim3 grid((unsigned)T.n_blocks, (unsigned)batch);
-    siddon_kernel<NDIM, ADJ><<<grid, T.tile_rows * T.tile_cols, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G,
-                                                                        nvox, T);
+    const int threads = T.tile_rows * T.tile_cols;
+    const bool mid = tiling == nullptr || tiling->voxel_rule == CTLAB_VOXEL_MIDPOINT;
+    const bool flat = tiling == nullptr || tiling->n_view == 0;
+    const int walk = tiling == nullptr ? CTLAB_WALK_AUTO : tiling->walk;
+    if constexpr (NDIM == 3) {
+        // Detector-row tilings (a warp = 32 rows of one column) may take the
+        // column-coherent walk; it checks per warp that the lanes share their
+        // x-y line and otherwise runs the per-lane walk.
+        if (!flat && T.tile_rows % 32 == 0 && walk == CTLAB_WALK_COLUMN) {
+            if (mid)
+                siddon3d_column_kernel<ADJ, true>
+                    <<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+            else
+                siddon3d_column_kernel<ADJ, false>
+                    <<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+            return launch_status(what);
+        }
+    }
+    if (mid)
+        siddon_kernel<NDIM, ADJ, true><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+    else
+        siddon_kernel<NDIM, ADJ, false><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
     return launch_status(what);
 }
 
@@ -249,7 +612,7 @@ using namespace ctlab;
 extern "C" int ctlab_forward_project_3d_on_the_fly_ex(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
                                                       int64_t n_z, const float* src, const float* dst,
                                                       int64_t n_ray, const float* M_inv, const float* b, float* out,
-                                                      const ctlab_ray_tiling* tiling, void* stream) {
+                                                      const ctlab_ray_opts* tiling, void* stream) {
     clear_error();
     const int64_t dims[3] = {n_x, n_y, n_z};
     return launch_siddon<3, false>("forward_project_3d_on_the_fly", volume, out, batch, dims, src, dst, n_ray,
@@ -259,7 +622,7 @@ extern "C" int ctlab_forward_project_3d_on_the_fly_ex(const float* volume, int64
 extern "C" int ctlab_back_project_3d_on_the_fly_ex(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                                    const float* dst, const float* M_inv, const float* b, int64_t n_x,
                                                    int64_t n_y, int64_t n_z, float* out, int accumulate,
-                                                   const ctlab_ray_tiling* tiling, void* stream) {
+                                                   const ctlab_ray_opts* tiling, void* stream) {
     clear_error();
     const int64_t dims[3] = {n_x, n_y, n_z};
     return launch_siddon<3, true>("back_project_3d_on_the_fly", sino, out, batch, dims, src, dst, n_ray, M_inv, b,
@@ -283,7 +646,7 @@ extern "C" int ctlab_back_project_3d_on_the_fly(const float* sino, int64_t batch
 extern "C" int ctlab_forward_project_2d_siddon(const float* image, int64_t batch, int64_t n_row, int64_t n_col,
                                                const float* src, const float* dst, int64_t n_ray,
                                                const float* M_inv, const float* b, float* out,
-                                               const ctlab_ray_tiling* tiling, void* stream) {
+                                               const ctlab_ray_opts* tiling, void* stream) {
     clear_error();
     const int64_t dims[2] = {n_row, n_col};
     return launch_siddon<2, false>("forward_project_2d_siddon", image, out, batch, dims, src, dst, n_ray, M_inv, b,
@@ -292,7 +655,7 @@ extern "C" int ctlab_forward_project_2d_siddon(const float* image, int64_t batch
 
 extern "C" int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                             const float* dst, const float* M_inv, const float* b, int64_t n_row,
-                                            int64_t n_col, float* out, int accumulate, const ctlab_ray_tiling* tiling,
+                                            int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
                                             void* stream) {
     clear_error();
     const int64_t dims[2] = {n_row, n_col};

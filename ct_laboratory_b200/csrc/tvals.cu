@@ -491,8 +491,8 @@ static int run_tvals(const char* what, const float* in, float* out, int64_t batc
     rc = warp_grid(what, n_ray, batch, grid);
     if (rc) return rc;
     CTLAB_REQUIRE(n_int >= 1 && n_int < (1LL << 30), "%s: n_int out of range", what);
-    CTLAB_REQUIRE(in && out && M_inv && b, "%s: null data pointer", what);
-    CTLAB_REQUIRE(n_ray == 0 || (tvals && src && dst), "%s: null tvals/src/dst", what);
+    CTLAB_REQUIRE((ADJ ? out : in) && M_inv && b, "%s: null data pointer", what);
+    CTLAB_REQUIRE(n_ray == 0 || (tvals && src && dst && (ADJ ? in : out)), "%s: null tvals/src/dst/sinogram", what);
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (n_ray == 0) return CTLAB_OK;
@@ -514,8 +514,9 @@ static int run_compressed(const char* what, const float* in, float* out, int64_t
     rc = warp_grid(what, n_ray, batch, grid);
     if (rc) return rc;
     CTLAB_REQUIRE(n_int >= 1 && n_int < (1LL << 30), "%s: n_int out of range", what);
-    CTLAB_REQUIRE(in && out && M_inv && b, "%s: null data pointer", what);
-    CTLAB_REQUIRE(n_ray == 0 || (tq && t_start && t_scale && src && dst), "%s: null table/src/dst", what);
+    CTLAB_REQUIRE((ADJ ? out : in) && M_inv && b, "%s: null data pointer", what);
+    CTLAB_REQUIRE(n_ray == 0 || (tq && t_start && t_scale && src && dst && (ADJ ? in : out)),
+                  "%s: null table/src/dst/sinogram", what);
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (n_ray == 0) return CTLAB_OK;
@@ -553,7 +554,8 @@ static int run_march2d(const char* what, const float* in, float* out, int64_t ba
     int rc = check_grid(what, 2, dims, D, nvox);
     if (rc) return rc;
     CTLAB_REQUIRE(n_ray >= 0 && batch >= 1 && batch <= 65535, "%s: bad n_ray/batch", what);
-    CTLAB_REQUIRE(in && out && M_inv && b && (n_ray == 0 || (src && dst)), "%s: null pointer", what);
+    CTLAB_REQUIRE((ADJ ? out : in) && M_inv && b && (n_ray == 0 || (src && dst && (ADJ ? in : out))),
+                  "%s: null pointer", what);
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (n_ray == 0) return CTLAB_OK;

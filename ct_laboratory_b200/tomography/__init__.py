@@ -13,3 +13,4 @@ from .fanbeam_projector_2d import *  # noqa: F401,F403
 from .conebeam_projector_3d import *  # noqa: F401,F403
 from .staticct_projector_2d import *  # noqa: F401,F403
 from .staticct_projector_3d import *  # noqa: F401,F403
+from .gather import *  # noqa: F401,F403

@@ -7,6 +7,8 @@ dst)``).  ``tvals=None`` is an addition: it runs the table-free Siddon kernel
 """
 from __future__ import annotations
 
+import torch
+
 from .. import _C
 from .. import _native as N
 from ._common import inverse, require_cuda
@@ -48,10 +50,18 @@ def back_project_2d_cuda(sinogram, tvals, M, b, src, dst, n_row, n_col, tiling=N
     return out
 
 
+def _check(src, dst, M_inv, b, *data):
+    for t in (src, dst, M_inv, b, *data):
+        if t.dtype != torch.float32 or not t.is_contiguous() or not t.is_cuda:
+            raise RuntimeError("2-D Siddon: tensors must be C-contiguous float32 CUDA tensors")
+    if src.dim() != 2 or src.shape[1] != 2 or dst.shape != src.shape:
+        raise RuntimeError(f"src/dst must be [n_ray, 2] (got {tuple(src.shape)}, {tuple(dst.shape)})")
+
+
 def forward_project_2d_siddon(image, M_inv, b, src, dst, tiling=None):
     """Table-free 2-D Siddon forward, always batched [B, n_ray]."""
-    import torch
     img = image.contiguous()
+    _check(src, dst, M_inv, b, img)
     batch, n_row, n_col = (1, *img.shape) if img.dim() == 2 else img.shape
     n_ray = src.shape[0]
     out = torch.empty((batch, n_ray), device=img.device, dtype=torch.float32)
@@ -63,8 +73,8 @@ def forward_project_2d_siddon(image, M_inv, b, src, dst, tiling=None):
 
 def back_project_2d_siddon(sinogram, M_inv, b, src, dst, n_row, n_col, tiling=None):
     """Exact adjoint of forward_project_2d_siddon, always batched [B, R, C]."""
-    import torch
     sino = sinogram.contiguous()
+    _check(src, dst, M_inv, b, sino)
     batch, n_ray = (1, sino.shape[0]) if sino.dim() == 1 else sino.shape
     out = torch.empty((batch, n_row, n_col), device=sino.device, dtype=torch.float32)
     with torch.cuda.device(sino.device):

@@ -29,10 +29,12 @@ class CTProjector2DModule(torch.nn.Module):
         self.n_row, self.n_col = int(n_row), int(n_col)
         self.ray_tiling = ray_tiling
         self._minv = InverseCache()
-        self.register_buffer("M", M)
-        self.register_buffer("b", b)
-        self.register_buffer("src", src)
-        self.register_buffer("dst", dst)
+        # the kernels read raw pointers: keep contiguous float32 copies
+        f32 = lambda t: t.to(torch.float32).contiguous()  # noqa: E731
+        self.register_buffer("M", f32(M))
+        self.register_buffer("b", f32(b))
+        self.register_buffer("src", f32(src))
+        self.register_buffer("dst", f32(dst))
         self.precomputed_intersections = bool(precomputed_intersections)
         self._tvals = None
         if self.precomputed_intersections:

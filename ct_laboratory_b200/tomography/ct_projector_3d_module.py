@@ -16,6 +16,10 @@ Differences, none in results:
    reference module's encoder (compress_tvals_to_uint16 semantics).
  * M^-1 is computed once on the device and cached until M changes.
  * an optional ``ray_tiling`` launch hint (set by the cone-beam class).
+ * ``deterministic_adjoint=True`` (with a flat-panel table ``panels``, which
+   the cone-beam and StaticCT classes build) makes ``back_project`` and the
+   autograd backward gather per voxel: bitwise reproducible, the exact
+   transpose of the forward with the crossing voxel rule.
 """
 from __future__ import annotations
 
@@ -28,6 +32,7 @@ from ._common import InverseCache, require_cuda, voxel_diag_len
 from .ct_projector_3d_autograd import CTProjector3DFunction
 from .ct_projector_3d_cuda import back_project_3d_cuda, compute_intersections_3d_cuda
 from .ct_projector_3d_torch import compress_tvals_to_uint16, decompress_tvals_from_uint16
+from .gather import back_project_3d_gather_cuda
 
 __all__ = ["CTProjector3DModule", "precompute_tvals_stitched"]
 
@@ -45,7 +50,7 @@ def _trim_inf_columns(t: torch.Tensor) -> torch.Tensor:
 
 class CTProjector3DModule(torch.nn.Module):
     def __init__(self, n_x, n_y, n_z, M, b, src, dst, backend="cuda", device=None, precomputed_intersections=False,
-                 tvals=None, use_compression=True, ray_tiling=None):
+                 tvals=None, use_compression=True, ray_tiling=None, panels=None, deterministic_adjoint=False):
         super().__init__()
         if device is None:
             device = torch.device("cuda" if torch.cuda.is_available() else "cpu")
@@ -54,10 +59,16 @@ class CTProjector3DModule(torch.nn.Module):
         self.use_compression = use_compression
         self.ray_tiling = ray_tiling
         self._minv = InverseCache()
-        self.register_buffer("M", M)
-        self.register_buffer("b", b)
-        self.register_buffer("src", src)
-        self.register_buffer("dst", dst)
+        # the kernels read raw pointers: keep contiguous float32 copies
+        f32 = lambda t: t.to(torch.float32).contiguous()  # noqa: E731
+        self.register_buffer("M", f32(M))
+        self.register_buffer("b", f32(b))
+        self.register_buffer("src", f32(src))
+        self.register_buffer("dst", f32(dst))
+        self.panels = panels
+        self.deterministic_adjoint = bool(deterministic_adjoint)
+        if self.deterministic_adjoint and panels is None:
+            raise ValueError("deterministic_adjoint needs a flat-panel table (panels_from_grid)")
         self.tvals_uint16 = None
         self.tvals_start = None
         self.tvals_scale = None
@@ -89,11 +100,14 @@ class CTProjector3DModule(torch.nn.Module):
         super().to(*args, **kwargs)
         device = torch._C._nn._parse_to(*args, **kwargs)[0]
         if device is not None:
-            for name in ("tvals_uint16", "tvals_start", "tvals_scale", "tvals_full"):
+            for name in ("tvals_uint16", "tvals_start", "tvals_scale", "tvals_full", "panels"):
                 t = getattr(self, name, None)
                 if isinstance(t, torch.Tensor):
                     setattr(self, name, t.to(device))
         return self
+
+    def _panels(self):
+        return self.panels if (self.deterministic_adjoint and self._table()[0] is None) else None
 
     def _table(self):
         if self.tvals_uint16 is not None:
@@ -112,7 +126,7 @@ class CTProjector3DModule(torch.nn.Module):
         self._ensure_table_device(volume.device)
         t_main, t_start, t_scale = self._table()
         return CTProjector3DFunction.apply(volume, t_main, t_start, t_scale, self.M, self.b, self.src, self.dst,
-                                           self.backend, self.ray_tiling, self.M_inv)
+                                           self.backend, self.ray_tiling, self.M_inv, self._panels())
 
     def forward_project(self, volume):
         return self.forward(volume)
@@ -123,6 +137,9 @@ class CTProjector3DModule(torch.nn.Module):
         t_main, t_start, t_scale = self._table()
         tv = (t_main, t_start, t_scale) if t_start is not None else t_main
         with torch.no_grad():
+            if self._panels() is not None:
+                return back_project_3d_gather_cuda(sinogram, self.src, self.dst, self.M, self.b, self.n_x, self.n_y,
+                                                   self.n_z, self.panels, M_inv=self.M_inv)
             return back_project_3d_cuda(sinogram.contiguous(), tv, self.src, self.dst, self.M, self.b, self.n_x,
                                         self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
 

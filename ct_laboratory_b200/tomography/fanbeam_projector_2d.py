@@ -44,8 +44,8 @@ def build_fanbeam_2d_geometry(n_view, n_det, sid, sdd, det_spacing=1.0, angle_of
         dsts.append(d)
     if not srcs:
         return torch.empty((0, 2), dtype=torch.float32), torch.empty((0, 2), dtype=torch.float32)
-    src = torch.from_numpy(np.concatenate(srcs).astype(np.float32))
-    dst = torch.from_numpy(np.concatenate(dsts).astype(np.float32))
+    src = torch.from_numpy(np.ascontiguousarray(np.concatenate(srcs), dtype=np.float32))
+    dst = torch.from_numpy(np.ascontiguousarray(np.concatenate(dsts), dtype=np.float32))
     return src, dst
 
 

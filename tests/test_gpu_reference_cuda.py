@@ -48,6 +48,16 @@ def test_on_the_fly_vs_reference_kernels(ref, voxel):
     ours_b = _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, 48, 44, 36)
     theirs_b = ref.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, 48, 44, 36)
     assert rel_err(ours_b.cpu().numpy(), theirs_b.cpu().numpy()) < 1e-5
+    # per ray (one-hot sinograms, no atomic ordering): the segment weights of
+    # every ray agree with the reference kernel's
+    n_ray = src.shape[0]
+    for s0 in range(0, n_ray, 4096):
+        idx = torch.arange(s0, min(n_ray, s0 + 4096), 97, device=DEV)
+        oh = torch.zeros(idx.numel(), n_ray, device=DEV)
+        oh[torch.arange(idx.numel(), device=DEV), idx] = 1.0
+        a = _C.back_project_3d_on_the_fly_cuda(oh, src, dst, Mi, b, 48, 44, 36)
+        r_ = ref.back_project_3d_on_the_fly_cuda(oh, src, dst, Mi, b, 48, 44, 36)
+        assert float((a - r_).abs().max()) <= 1e-6 * float(r_.abs().max())
 
 
 @pytest.mark.parametrize("name", ["cone3d", "affine3d", "edge3d", "static3d", "kat3d"])
@@ -65,20 +75,33 @@ def test_tables_and_codecs_vs_reference_kernels(ref, name):
     for a, b_ in zip(c_o, c_r):
         assert torch.equal(a, b_), "compressed streams differ"
     vol, y = T(g["vol"]), T(g["y"])
+
+    def close(o, r):
+        # The reference's compressed kernels return NaN for a zero-length
+        # ray (src == dst: its all-inf row gives start = inf, and its
+        # `seg_len < 1e-9` test is false for NaN); ours return 0 there.
+        o, r = o.cpu().numpy(), r.cpu().numpy()
+        nan = np.isnan(r)
+        if nan.any():
+            assert np.any(np.all(g["src"] == g["dst"], axis=1)), "NaN without a zero-length ray"
+            assert not np.isnan(o).any()
+            o, r = o[~nan], r[~nan]
+        return rel_err(o, r) < 1e-5
+
     for fo, fr in ((_C.forward_project_3d_cuda(vol, tv_r, src, dst, Mi, b),
                     ref.forward_project_3d_cuda(vol, tv_r, src, dst, Mi, b)),
                    (_C.forward_project_3d_compressed_cuda(vol, *c_r, src, dst, Mi, b),
                     ref.forward_project_3d_compressed_cuda(vol, *c_r, src, dst, Mi, b)),
                    (_C.forward_project_3d_on_the_fly_cuda(vol, src, dst, Mi, b),
                     ref.forward_project_3d_on_the_fly_cuda(vol, src, dst, Mi, b))):
-        assert rel_err(fo.cpu().numpy(), fr.cpu().numpy()) < 1e-5
+        assert close(fo, fr)
     for bo, br in ((_C.back_project_3d_cuda(y, tv_r, src, dst, Mi, b, *d),
                     ref.back_project_3d_cuda(y, tv_r, src, dst, Mi, b, *d)),
                    (_C.back_project_3d_compressed_cuda(y, *c_r, src, dst, Mi, b, *d),
                     ref.back_project_3d_compressed_cuda(y, *c_r, src, dst, Mi, b, *d)),
                    (_C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, *d),
                     ref.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, *d))):
-        assert rel_err(bo.cpu().numpy(), br.cpu().numpy()) < 1e-5
+        assert close(bo, br)
 
 
 @pytest.mark.parametrize("name", ["kat2d", "fan2d", "static2d"])
