@@ -197,7 +197,7 @@ extern "C" int ctlab_back_project_3d_gather(const float* sino, int64_t batch, in
     const char* what = "back_project_3d_gather";
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535]", what);
     CTLAB_REQUIRE(n_ray >= 0 && n_panel >= 0 && n_panel < (1LL << 31), "%s: bad n_ray/n_panel", what);
-    CTLAB_REQUIRE(n_x >= 1 && n_y >= 1 && n_z >= 1 && n_x < (1 << 24) && n_y < (1 << 24) && n_z < (1 << 24),
+    CTLAB_REQUIRE(n_x >= 1 && n_y >= 1 && n_z >= 1 && n_x <= (1 << 22) && n_y <= (1 << 22) && n_z <= (1 << 22),
                   "%s: bad grid", what);
     const int64_t nvox = n_x * n_y * n_z;
     CTLAB_REQUIRE(nvox < (1LL << 31), "%s: volume too large", what);

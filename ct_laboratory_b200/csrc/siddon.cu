@@ -38,6 +38,15 @@ struct GridDims {
     int stride[NDIM];
 };
 
+// Round half to even to int without a conversion instruction: adding
+// 1.5*2^23 leaves the rounded integer in the low mantissa bits (exact for
+// |x| < 2^22); outside that range (and for NaN / inf) the result is an
+// integer >= 2^22 or negative, which every grid bound check (n <= 2^22)
+// rejects.
+__device__ __forceinline__ int rne_int(float x) {
+    return __float_as_int(__fadd_rn(x, 12582912.0f)) - 0x4B400000;
+}
+
 // Voxel of a segment [t0, t1] under the reference's rule: the world-space
 // midpoint s + t_mid*v mapped to index space and rounded half to even
 // (ct_projector_3d.cu:982-996).  Returns the flat index or -1 (outside).
@@ -54,8 +63,8 @@ __device__ __forceinline__ int midpoint_voxel(const AffineT<NDIM>& A, const floa
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < NDIM; ++a) {
-        const int i = __float2int_rn(f[a]);
-        ok = ok && i >= 0 && i < G.n[a];
+        const int i = rne_int(f[a]);
+        ok = ok && (unsigned)i < (unsigned)G.n[a];
         flat += i * G.stride[a];
     }
     return ok ? flat : -1;
@@ -151,19 +160,29 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
         tn[a] = plane_t(pn[a], s[a], inv[a]);
     }
 
-    // The merge walk.  Every plane is crossed at most once, which bounds the
-    // loop even for non-finite input.
+    // The merge walk.  Each step ends the current segment at the nearest
+    // next plane (or at t_exit) and then steps every axis whose next plane
+    // lies exactly there: equal plane parameters of two axes only ever bound
+    // a zero-length segment, which the reference skips and which would add
+    // nothing here, so stepping them together gives the same segments.  The
+    // steps are predicated, not branched, so the lanes of a warp never
+    // diverge inside the walk.
+    //
+    // The voxel index never leaves the grid: an axis is stepped across its
+    // last plane only when that plane's parameter (>= t_exit, which is the
+    // minimum over the axes' exit planes) is below t_exit, which cannot
+    // happen.  Every plane is crossed at most once, which bounds the loop
+    // even for non-finite input.
     int max_it = 3;
 #pragma unroll
     for (int a = 0; a < NDIM; ++a) max_it += G.n[a];
-    float acc = 0.f;
+    (void)nvox;
     float t_cur = t_enter;
-    if constexpr (!ADJ && !MID) {
-        // Forward, crossing rule: walk four segments, then issue their four
-        // gathers back to back and accumulate them in walk order (the sum is
-        // the same sequence of fused multiply-adds as one at a time, so the
-        // result is bitwise that of the loop below).  Four loads in flight
-        // per lane instead of one hides the L2 latency of the gathers.
+    if constexpr (!ADJ) {
+        // Forward: four steps, then their four gathers back to back (four
+        // loads in flight per lane), accumulated in walk order; zero-length
+        // segments (ties, and the padding after the exit) are not added.
+        float acc = 0.f;
         bool done = false;
 #pragma unroll 1
         for (int it = 0; it < max_it && !done; it += 4) {
@@ -171,83 +190,61 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             float sq[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                vq[q] = 0;
-                sq[q] = 0.f;
-                if (done) continue;
                 float tm = tn[0];
 #pragma unroll
                 for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
-                const bool fin = !(tm < t_exit);
-                const float t1 = fin ? t_exit : tm;
-                if (t1 > t_cur && (unsigned)idx < nvox) {
-                    vq[q] = idx;
-                    sq[q] = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                const float t1 = fminf(tm, t_exit);
+                float seg = done ? 0.f : __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                int v = idx;
+                if constexpr (MID) {
+                    const int m = midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G);
+                    v = m < 0 ? 0 : m;
+                    seg = m < 0 ? 0.f : seg;
                 }
-                done = fin;
-                if (!fin) {
-                    t_cur = t1;
-                    if (tn[0] == tm) {
-                        idx += ds[0];
-                        pn[0] += ps[0];
-                        tn[0] = plane_t(pn[0], s[0], inv[0]);
-                    } else if (NDIM == 2 || tn[1] == tm) {
-                        idx += ds[1];
-                        pn[1] += ps[1];
-                        tn[1] = plane_t(pn[1], s[1], inv[1]);
-                    } else {
-                        idx += ds[NDIM - 1];
-                        pn[NDIM - 1] += ps[NDIM - 1];
-                        tn[NDIM - 1] = plane_t(pn[NDIM - 1], s[NDIM - 1], inv[NDIM - 1]);
+                vq[q] = v;
+                sq[q] = seg;
+                done = done || !(tm < t_exit);
+                t_cur = t1;
+#pragma unroll
+                for (int a = 0; a < NDIM; ++a) {
+                    if (!done && tn[a] == tm) {
+                        idx += ds[a];
+                        pn[a] += ps[a];
+                        tn[a] = plane_t(pn[a], s[a], inv[a]);
                     }
                 }
             }
             float vv[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) vv[q] = sq[q] != 0.f ? __ldg(vol + vq[q]) : 0.f;
+            for (int q = 0; q < 4; ++q) vv[q] = __ldg(vol + vq[q]);
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (sq[q] != 0.f) acc = __fmaf_rn(vv[q], sq[q], acc);
+            for (int q = 0; q < 4; ++q) acc = sq[q] > 0.f ? __fmaf_rn(vv[q], sq[q], acc) : acc;
         }
         return acc;
-    }
+    } else {
 #pragma unroll 1
-    for (int it = 0; it < max_it; ++it) {
-        float tm = tn[0];
+        for (int it = 0; it < max_it; ++it) {
+            float tm = tn[0];
 #pragma unroll
-        for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
-        const bool fin = !(tm < t_exit);
-        const float t1 = fin ? t_exit : tm;
-        if (t1 > t_cur) {
+            for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
+            const float t1 = fminf(tm, t_exit);
+            // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
+            const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
             const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
-            if ((unsigned)v < nvox) {
-                // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
-                const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
-                if constexpr (ADJ) {
-                    atomicAdd(out + v, __fmul_rn(y, seg));
-                } else {
-                    acc = __fmaf_rn(__ldg(vol + v), seg, acc);
+            if (seg > 0.f && v >= 0) atomicAdd(out + v, __fmul_rn(y, seg));
+            if (!(tm < t_exit)) break;
+            t_cur = t1;
+#pragma unroll
+            for (int a = 0; a < NDIM; ++a) {
+                if (tn[a] == tm) {
+                    idx += ds[a];
+                    pn[a] += ps[a];
+                    tn[a] = plane_t(pn[a], s[a], inv[a]);
                 }
             }
         }
-        if (fin) break;
-        t_cur = t1;
-        // Advance the axis that owns tm (x before y before z on ties, the
-        // order in which equal values leave the reference's sort).
-        if (tn[0] == tm) {
-            idx += ds[0];
-            pn[0] += ps[0];
-            tn[0] = plane_t(pn[0], s[0], inv[0]);
-        } else if (NDIM == 2 || tn[1] == tm) {
-            idx += ds[1];
-            pn[1] += ps[1];
-            tn[1] = plane_t(pn[1], s[1], inv[1]);
-        } else {
-            idx += ds[NDIM - 1];
-            pn[NDIM - 1] += ps[NDIM - 1];
-            tn[NDIM - 1] = plane_t(pn[NDIM - 1], s[NDIM - 1], inv[NDIM - 1]);
-        }
+        return 0.f;
     }
-    return acc;
 }
 
 template <int NDIM, bool ADJ, bool MID>
@@ -553,7 +550,7 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     GridDims<NDIM> G;
     int64_t nvox = 1;
     for (int a = 0; a < NDIM; ++a) {
-        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] < (1 << 24), "%s: grid dimension %d out of range (%lld)", what, a,
+        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] <= (1 << 22), "%s: grid dimension %d out of range (%lld)", what, a,
                       (long long)dims[a]);
         nvox *= dims[a];
     }

@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(256) march2d_kernel(const float* __restrict__ 
 static int check_grid(const char* what, int ndim, const int64_t* dims, Dims& D, int64_t& nvox) {
     nvox = 1;
     for (int a = 0; a < ndim; ++a) {
-        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] < (1 << 24), "%s: grid dimension %d out of range (%lld)", what, a,
+        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] <= (1 << 22), "%s: grid dimension %d out of range (%lld)", what, a,
                       (long long)dims[a]);
         D.n[a] = (int)dims[a];
         nvox *= dims[a];

@@ -1,0 +1,376 @@
+"""Matrix-free leading eigenpairs of G = A^T A and the preconditioners built on them.
+
+Mirrors the reference's sparse_eigen_preconditioner area
+(ct_laboratory/sparse_eigen_preconditioner/sparse_eigen_decomposition.py:39-366,
+preconditioners.py:28-138): ``SparseEigenDecomposition(projector, k)`` with
+``compute_weights(method=...)`` filling buffers ``s`` (singular values,
+descending), ``v`` (N x k image eigenvectors) and ``p`` (n_ray x k
+projection eigenvectors A v), ``save`` / ``load``, ``register_method``,
+``to_image_preconditioner`` / ``to_projection_preconditioner``; and the
+image- and projection-domain preconditioners
+    P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I.
+
+Solvers:
+  "subspace"  block power iteration + Rayleigh-Ritz, as the reference's
+  "eigsh"     SciPy ARPACK with the matvec on the GPU (one host round trip
+              per matvec, as the reference's)
+  "lanczos"   thick-restart Lanczos with full re-orthogonalisation, entirely
+              on the GPU: no host round trip per matvec.
+The Gram operator is applied to a block of columns with one batched forward
+and one batched adjoint launch (the reference applies it column by column,
+sparse_eigen_decomposition.py:120-128).
+"""
+from __future__ import annotations
+
+import time
+
+import torch
+from torch import nn
+
+from .optimization import Preconditioner
+
+__all__ = ["SparseEigenDecomposition", "SparseEigenImagePreconditioner", "SparseEigenProjectionPreconditioner"]
+
+
+class SparseEigenDecomposition(nn.Module):
+    _METHODS = {}
+
+    def __init__(self, operator=None, k=32, volume_shape=None, gram=None, dtype=None, device=None, block=None):
+        super().__init__()
+        self.k = int(k)
+        self._projector = None
+        self._forward = None
+        self._gram_user = gram
+        self.block = block  # columns per batched Gram application (None: all at once)
+        if gram is None and operator is None:
+            raise ValueError("provide either an `operator` (projector or forward callable) or a `gram` callable")
+        if hasattr(operator, "forward_project") and hasattr(operator, "back_project"):
+            self._projector = operator
+            self._forward = operator.forward_project
+            volume_shape = (operator.n_x, operator.n_y, operator.n_z)
+            if device is None and hasattr(operator, "M"):
+                device = operator.M.device
+        elif callable(operator):
+            if volume_shape is None and gram is None:
+                raise ValueError("`volume_shape` is required when `operator` is a bare forward callable")
+            self._forward = operator
+        self.volume_shape = tuple(volume_shape) if volume_shape is not None else None
+        self.dtype = dtype or torch.float32
+        self.device_ = device or torch.device("cpu")
+        self.register_buffer("s", torch.zeros(0, dtype=self.dtype))
+        self.register_buffer("v", torch.zeros(0, 0, dtype=self.dtype))
+        self.register_buffer("p", torch.zeros(0, dtype=self.dtype))
+        self.n_matvec = 0
+
+    # -- operator plumbing ---------------------------------------------------
+    @property
+    def N(self):
+        if self.volume_shape is not None:
+            n = 1
+            for d in self.volume_shape:
+                n *= d
+            return n
+        return self.v.shape[0] if self.v.numel() else None
+
+    def _apply_gram(self, x):
+        """G x for one flattened vector."""
+        self.n_matvec += 1
+        if self._gram_user is not None:
+            return self._gram_user(x).reshape(-1)
+        vol = x.contiguous().reshape(self.volume_shape)
+        with torch.no_grad():
+            return self._projector.back_project(self._projector.forward_project(vol)).reshape(-1)
+
+    def _gram_matmul(self, Q, use_tqdm=False, desc="G @ Q"):
+        """G applied to every column of Q (N x m): the columns go through the
+        projector as one batch of volumes."""
+        if self._gram_user is not None or self._projector is None:
+            return torch.stack([self._apply_gram(Q[:, j]) for j in range(Q.shape[1])], dim=1)
+        m = Q.shape[1]
+        step = m if self.block is None else max(1, int(self.block))
+        out = torch.empty_like(Q)
+        for a in range(0, m, step):
+            bcols = Q[:, a:a + step].t().contiguous().reshape(-1, *self.volume_shape)
+            with torch.no_grad():
+                g = self._projector.back_project(self._projector.forward_project(bcols))
+            out[:, a:a + step] = g.reshape(bcols.shape[0], -1).t()
+            self.n_matvec += bcols.shape[0]
+        return out
+
+    # -- solvers ---------------------------------------------------------------
+    def _solve_subspace(self, gram, N, k, n_iters=30, tol=1e-6, seed=None, oversample=0, verbose=False,
+                        use_tqdm=False):
+        """Block power iteration + Rayleigh-Ritz (reference :140-183)."""
+        gen = None
+        if seed is not None:
+            gen = torch.Generator(device=self.device_).manual_seed(int(seed))
+        m = min(N, k + max(0, int(oversample)))
+        Q = torch.randn(N, m, dtype=self.dtype, device=self.device_, generator=gen)
+        Q, _ = torch.linalg.qr(Q)
+        prev = None
+        for it in range(int(n_iters)):
+            Z = gram(Q)
+            Q, _ = torch.linalg.qr(Z)
+            T = Q.t() @ gram(Q)
+            T = 0.5 * (T + T.t())
+            ritz = torch.linalg.eigvalsh(T)
+            if prev is not None:
+                rel = (ritz - prev).abs().max() / (prev.abs().max() + 1e-30)
+                if verbose:
+                    print(f"  [subspace] iter {it:03d}  max Ritz={float(ritz.max()):.4e}  rel-change={float(rel):.2e}")
+                if rel < tol:
+                    break
+            prev = ritz
+        GQ = gram(Q)
+        T = Q.t() @ GQ
+        T = 0.5 * (T + T.t())
+        evals, W = torch.linalg.eigh(T)
+        idx = torch.argsort(evals, descending=True)[:k]
+        return torch.clamp(evals[idx], min=0.0), Q @ W[:, idx]
+
+    def _solve_eigsh(self, gram, N, k, tol=1e-3, maxiter=5000, seed=42, ncv=None, verbose=False, use_tqdm=False,
+                     **_ignored):
+        """SciPy ARPACK ("LM") with the Gram matvec on the GPU (reference :185-224)."""
+        import numpy as np
+        from scipy.sparse.linalg import LinearOperator, eigsh
+
+        dev, dt = self.device_, self.dtype
+
+        def matvec(x):
+            xt = torch.as_tensor(np.asarray(x), dtype=dt, device=dev)
+            return self._apply_gram(xt).to("cpu", torch.float32).numpy()
+
+        op = LinearOperator((N, N), matvec=matvec, dtype=np.float32)
+        rng = np.random.default_rng(int(seed) if seed is not None else None)
+        v0 = rng.standard_normal(N).astype(np.float32)
+        ncv = ncv if ncv is not None else min(N - 1, max(20, 2 * k + 1))
+        s2_np, V_np = eigsh(op, k=k, which="LM", ncv=ncv, v0=v0, tol=tol, maxiter=maxiter)
+        order = np.argsort(s2_np)[::-1]
+        s2 = torch.as_tensor(np.clip(s2_np[order], 0.0, None).copy(), dtype=dt, device=dev)
+        V = torch.as_tensor(V_np[:, order].copy(), dtype=dt, device=dev)
+        return s2, V
+
+    def _solve_lanczos(self, gram, N, k, tol=1e-3, ncv=None, max_restarts=50, seed=42, verbose=False,
+                       use_tqdm=False, **_ignored):
+        """Thick-restart Lanczos for the k largest eigenpairs, on the device.
+
+        Basis V (N x (ncv+1)) in float32 with two passes of classical
+        Gram-Schmidt against all previous vectors per step; the projected
+        matrix T = V^T G V in float64.  After ncv vectors the k leading Ritz
+        vectors and the residual direction are kept and the iteration
+        continues from them (thick restart).  Converged when every kept Ritz
+        pair has residual |beta * s_last| <= tol * theta_max."""
+        dev, dt = self.device_, self.dtype
+        ncv = int(ncv) if ncv is not None else min(N - 1, max(20, 2 * k + 1))
+        if not (k < ncv < N):
+            raise ValueError("lanczos needs k < ncv < N")
+        gen = torch.Generator(device="cpu").manual_seed(int(seed))
+        V = torch.empty(N, ncv + 1, dtype=dt, device=dev)
+        v0 = torch.randn(N, generator=gen, dtype=dt).to(dev)
+        V[:, 0] = v0 / v0.norm()
+        T = torch.zeros(ncv, ncv, dtype=torch.float64, device=dev)
+        start = 0
+        beta_last = 0.0
+        for restart in range(int(max_restarts)):
+            for j in range(start, ncv):
+                w = self._apply_gram(V[:, j])
+                h = V[:, :j + 1].t() @ w
+                w = w - V[:, :j + 1] @ h
+                h2 = V[:, :j + 1].t() @ w
+                w = w - V[:, :j + 1] @ h2
+                h = (h + h2).double()
+                T[:j + 1, j] = h
+                T[j, :j + 1] = h
+                beta = w.norm()
+                if j + 1 < ncv:
+                    T[j + 1, j] = T[j, j + 1] = beta.double()
+                V[:, j + 1] = w / beta.clamp_min(1e-30)
+                beta_last = beta
+            theta, S = torch.linalg.eigh(T)
+            order = torch.argsort(theta, descending=True)
+            theta, S = theta[order], S[:, order]
+            res = (beta_last.double() * S[-1, :k]).abs()
+            if verbose:
+                print(f"  [lanczos] restart {restart}: theta_max={float(theta[0]):.4e} "
+                      f"max residual/theta_max={float(res.max() / theta[0].abs()):.2e}")
+            if bool((res <= tol * theta[0].abs()).all()) or restart == max_restarts - 1:
+                break
+            # thick restart: keep k Ritz vectors and the residual direction
+            Y = V[:, :ncv] @ S[:, :k].to(dt)
+            resid = V[:, ncv].clone()
+            V[:, :k] = Y
+            V[:, k] = resid
+            T.zero_()
+            T[:k, :k] = torch.diag(theta[:k])
+            coup = beta_last.double() * S[-1, :k]
+            T[k, :k] = coup
+            T[:k, k] = coup
+            start = k
+        Y = V[:, :ncv] @ S[:, :k].to(dt)
+        return torch.clamp(theta[:k], min=0.0).to(dt), Y
+
+    # -- public API --------------------------------------------------------------
+    def compute_weights(self, k=None, method="subspace", compute_projection_basis=None, verbose=False,
+                        use_tqdm=False, **kwargs):
+        if k is not None:
+            self.k = int(k)
+        k = self.k
+        N = self.N
+        if N is None:
+            raise RuntimeError("cannot infer problem size N; give volume_shape or gram")
+        solver = self._METHODS.get(method)
+        if solver is None:
+            raise KeyError(f"unknown method '{method}'; registered: {sorted(self._METHODS)}")
+        t0 = time.time()
+        s2, V = solver(self, self._gram_matmul, N, k, verbose=verbose, use_tqdm=use_tqdm, **kwargs)
+        s = torch.sqrt(torch.clamp(s2, min=0.0)).to(self.dtype)
+        self.register_buffer("s", s.contiguous())
+        self.register_buffer("v", V.to(self.dtype).contiguous())
+        if compute_projection_basis is None:
+            compute_projection_basis = self._forward is not None and self._projector is not None
+        if compute_projection_basis:
+            if self._forward is None:
+                raise RuntimeError("projection basis requested but no forward operator")
+            with torch.no_grad():
+                vols = self.v.t().contiguous().reshape(-1, *self.volume_shape)
+                p = self._forward(vols)
+            self.register_buffer("p", p.reshape(vols.shape[0], -1).t().contiguous())
+        else:
+            self.register_buffer("p", torch.zeros(0, dtype=self.dtype))
+        if verbose:
+            print(f"[SparseEigenDecomposition] {method} done in {time.time() - t0:.2f}s, {self.n_matvec} matvecs")
+        return self
+
+    @property
+    def eigenvalues(self):
+        return self.s ** 2
+
+    def to_image_preconditioner(self, eps=1e-12):
+        self._require_computed()
+        return SparseEigenImagePreconditioner(self.s, self.v, eps=eps)
+
+    def to_projection_preconditioner(self, projector=None, eps=1e-12, chunk=None):
+        self._require_computed()
+        if self.p.numel() == 0:
+            raise RuntimeError("projection basis not available; recompute with compute_projection_basis=True")
+        projector = projector or self._projector
+        if projector is None:
+            raise ValueError("a projector is required to build a projection preconditioner")
+        return SparseEigenProjectionPreconditioner(projector, self.p, self.eigenvalues, eps=eps, chunk=chunk)
+
+    def _require_computed(self):
+        if self.v.numel() == 0:
+            raise RuntimeError("no eigen-basis; call compute_weights() or load() first")
+
+    def _load_from_state_dict(self, state_dict, prefix, *args, **kwargs):
+        for name in ("s", "v", "p"):
+            key = prefix + name
+            if key in state_dict:
+                self.register_buffer(name, torch.empty_like(state_dict[key]))
+        return super()._load_from_state_dict(state_dict, prefix, *args, **kwargs)
+
+    def save(self, path):
+        torch.save({"state_dict": self.state_dict(), "k": self.k, "volume_shape": self.volume_shape}, path)
+        return path
+
+    def load(self, path, map_location=None):
+        ckpt = torch.load(path, map_location=map_location or self.device_)
+        if isinstance(ckpt, dict) and "state_dict" in ckpt:
+            self.k = ckpt.get("k", self.k)
+            if ckpt.get("volume_shape") is not None:
+                self.volume_shape = tuple(ckpt["volume_shape"])
+            state = ckpt["state_dict"]
+        else:
+            state = ckpt
+        self.load_state_dict(state)
+        return self
+
+    @classmethod
+    def register_method(cls, name, fn):
+        cls._METHODS[name] = fn
+        return fn
+
+
+SparseEigenDecomposition.register_method("subspace", SparseEigenDecomposition._solve_subspace)
+SparseEigenDecomposition.register_method("eigsh", SparseEigenDecomposition._solve_eigsh)
+SparseEigenDecomposition.register_method("lanczos", SparseEigenDecomposition._solve_lanczos)
+
+
+class SparseEigenImagePreconditioner(Preconditioner):
+    """P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I on flattened volumes
+    (reference preconditioners.py:28-57)."""
+
+    def __init__(self, s, v, eps=1e-12):
+        super().__init__()
+        self.register_buffer("v", v)
+        s_min = s.min()
+        self.register_buffer("diag_fwd", 1.0 / (s + eps) - 1.0 / (s_min + eps))
+        self.register_buffer("diag_inv", (s - s_min))
+        self.register_buffer("inv_s_min", 1.0 / (s_min + eps))
+        self.register_buffer("s_min", s_min.clone())
+
+    def forward(self, x):
+        xf = x.reshape(-1)
+        c = torch.mv(self.v.t(), xf) * self.diag_fwd
+        return torch.mv(self.v, c) + self.inv_s_min * xf
+
+    def inverse(self, x):
+        xf = x.reshape(-1)
+        c = torch.mv(self.v.t(), xf) * self.diag_inv
+        return torch.mv(self.v, c) + self.s_min * xf
+
+
+class SparseEigenProjectionPreconditioner(Preconditioner):
+    """The same P through the projection basis p = A V and the projector
+    (reference preconditioners.py:60-138)."""
+
+    def __init__(self, projector, p, s2, eps=1e-12, chunk=None):
+        super().__init__()
+        self.projector = projector
+        self.nx, self.ny, self.nz = projector.n_x, projector.n_y, projector.n_z
+        self.dev = projector.M.device
+        self.register_buffer("p", p)
+        s2 = s2.to(self.dev)
+        s = torch.sqrt(torch.clamp(s2, min=0.0))
+        s_min = s.min()
+        s4 = torch.clamp(s2, min=eps).pow(2)
+        self.register_buffer("w_fwd", (1.0 / (s + eps) - 1.0 / (s_min + eps)) / s4)
+        self.register_buffer("w_inv", (s - s_min) / s4)
+        self.register_buffer("inv_s_min", 1.0 / (s_min + eps))
+        self.register_buffer("s_min", s_min.clone())
+        self.chunk = chunk
+
+    def _pk_T(self, r):
+        r = r.reshape(-1)
+        p = self.p.to(self.dev)
+        if self.chunk is None:
+            return torch.mv(p.t(), r.to(p.dtype))
+        out = torch.empty(p.shape[1], device=self.dev)
+        for a in range(0, p.shape[1], self.chunk):
+            out[a:a + self.chunk] = torch.mv(p[:, a:a + self.chunk].t(), r)
+        return out
+
+    def _pk(self, c):
+        p = self.p.to(self.dev)
+        if self.chunk is None:
+            return torch.mv(p, c.to(self.dev))
+        out = None
+        for a in range(0, p.shape[1], self.chunk):
+            part = torch.mv(p[:, a:a + self.chunk], c[a:a + self.chunk])
+            out = part if out is None else out + part
+        return out
+
+    def _apply(self, x, w):
+        xf = x.reshape(-1)
+        ax = self.projector.forward_project(xf.view(self.nx, self.ny, self.nz))
+        c = self._pk_T(ax.reshape(-1)) * w
+        proj = self._pk(c).view(ax.shape)
+        return self.projector.back_project(proj).reshape(-1)
+
+    def forward(self, x):
+        xf = x.reshape(-1)
+        return self._apply(xf, self.w_fwd) + self.inv_s_min * xf
+
+    def inverse(self, x):
+        xf = x.reshape(-1)
+        return self._apply(xf, self.w_inv) + self.s_min * xf
