@@ -119,6 +119,41 @@ __device__ __forceinline__ void world_to_index2(const Affine2& A, float x, float
 // reciprocal-multiply form of collect_hits (ct_projector_3d.cu:866-868).
 __device__ __forceinline__ float plane_t(float p, float s, float inv) { return __fmul_rn(__fsub_rn(p, s), inv); }
 
+// Returns `p` as an opaque register value.  Inside a hot loop the compiler
+// may otherwise re-derive a base pointer from the kernel parameters at every
+// use (constant-bank loads plus 64-bit address arithmetic per access).
+template <typename T>
+__device__ __forceinline__ T* pin_ptr(T* p) {
+    asm volatile("" : "+l"(p));
+    return p;
+}
+
+// L2 eviction policies.  The volume is gathered over and over while the
+// ray geometry and the sinogram stream through once; marking the volume
+// evict-last and the streams evict-first keeps a volume of up to about half
+// the 126 MB L2 resident while hundreds of MB of geometry pass by.
+__device__ __forceinline__ uint64_t l2_policy_keep() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ void st_stream(float* p, float v) { __stcs(p, v); }
+
+// red.global.add.f32 issued under a predicate: the reduction is one
+// predicated instruction instead of a branch around an atomicAdd.
+__device__ __forceinline__ void red_add_if(float* addr, float v, bool pred) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t@p red.global.add.f32 [%0], %1;\n\t}" ::"l"(addr), "f"(v),
+        "r"((int)pred)
+        : "memory");
+}
+
 // Ray tiling resolved on the host into plain integers for the kernels.
 struct Tiling {
     int64_t n_view, n_row, n_col;
@@ -132,15 +167,23 @@ struct Tiling {
 int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& out);
 
 // Ray handled by this thread, or -1 when the thread's slot is outside the grid.
+//
+// Blocks are numbered band-major: row tile outermost, then view, then column
+// tile.  Blocks run roughly in index order, so the blocks resident at any
+// moment share one band of detector rows across many views; for a cone-beam
+// scan such a band sees a slab of the volume about tile_rows detector rows
+// thick, and the volume voxels the whole GPU touches at a time stay a small,
+// L2-resident fraction of the volume.  The launch has at most 2^31 - 1
+// blocks, so all tile coordinates fit 32-bit unsigned division.
 __device__ __forceinline__ int64_t tile_ray(const Tiling& T) {
-    int64_t blk = blockIdx.x;
-    int64_t per_view = T.tiles_r * T.tiles_c;
-    int64_t view = blk / per_view;
-    int64_t rem = blk - view * per_view;
-    int64_t tr = rem / T.tiles_c;
-    int64_t tc = rem - tr * T.tiles_c;
-    int lane_r = threadIdx.x % T.tile_rows;
-    int lane_c = threadIdx.x / T.tile_rows;
+    const unsigned blk = blockIdx.x;
+    const unsigned per_band = (unsigned)(T.n_view * T.tiles_c);
+    const unsigned tr_u = blk / per_band;
+    const unsigned rem = blk - tr_u * per_band;
+    const unsigned view_u = rem / (unsigned)T.tiles_c;
+    const int64_t view = view_u, tr = tr_u, tc = rem - view_u * (unsigned)T.tiles_c;
+    const int lane_r = threadIdx.x % T.tile_rows;
+    const int lane_c = threadIdx.x / T.tile_rows;
     int64_t row = tr * T.tile_rows + lane_r;
     int64_t col = tc * T.tile_cols + lane_c;
     if (row >= T.n_row || col >= T.n_col) return -1;

@@ -15,9 +15,10 @@
 // the segment midpoint; the two agree except for segments of rounding-noise
 // length, which contribute rounding-noise amounts.
 //
-// Memory behaviour: the volume is read through the read-only path (__ldg)
-// and, at the benchmark size (256^3 fp32 = 64 MiB), stays resident in the
-// 126 MB L2.  A CTA covers `tile_rows` detector rows x (threads/tile_rows)
+// Memory behaviour: the volume is read through the read-only path with an
+// L2 evict-last policy and the ray geometry and sinogram stream through with
+// evict-first, so that a volume the size of the benchmark's (256^3 fp32 =
+// 64 MiB) stays resident in the 126 MB L2.  A CTA covers `tile_rows` detector rows x (threads/tile_rows)
 // columns, with warp lanes along rows, so that for a cone-beam scan the 32
 // lanes of a warp trace 32 vertically adjacent rays: they share the same x-y
 // path and touch neighbouring k (fastest-varying) voxels, so a warp's gather
@@ -184,6 +185,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
         // segments (ties, and the padding after the exit) are not added.
         float acc = 0.f;
         bool done = false;
+        const uint64_t pol = l2_policy_keep();
 #pragma unroll 1
         for (int it = 0; it < max_it && !done; it += 4) {
             int vq[4];
@@ -216,7 +218,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             }
             float vv[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) vv[q] = __ldg(vol + vq[q]);
+            for (int q = 0; q < 4; ++q) vv[q] = ld_keep(vol + (unsigned)vq[q], pol);
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc = sq[q] > 0.f ? __fmaf_rn(vv[q], sq[q], acc) : acc;
         }
@@ -231,7 +233,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
             const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
             const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
-            if (seg > 0.f && v >= 0) atomicAdd(out + v, __fmul_rn(y, seg));
+            red_add_if(out + (unsigned)v, __fmul_rn(y, seg), seg > 0.f && v >= 0);
             if (!(tm < t_exit)) break;
             t_cur = t1;
 #pragma unroll
@@ -265,61 +267,79 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
     float sw[NDIM], dw[NDIM];
 #pragma unroll
     for (int a = 0; a < NDIM; ++a) {
-        sw[a] = __ldg(src + r * NDIM + a);
-        dw[a] = __ldg(dst + r * NDIM + a);
+        sw[a] = ld_stream(src + r * NDIM + a);
+        dw[a] = ld_stream(dst + r * NDIM + a);
     }
     if constexpr (ADJ) {
-        const float y = __ldg(in + bi * n_ray + r);
+        const float y = ld_stream(in + bi * n_ray + r);
         if (y == 0.f) return;  // contributes exactly nothing
         traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
     } else {
-        out[bi * n_ray + r] =
-            traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox);
+        st_stream(out + bi * n_ray + r,
+                  traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox));
     }
 }
 
 // ----------------------------------------------------------------------------
-// Column-coherent 3-D traversal.
+// Shared x-y walk for detector columns (3-D, crossing rule).
 //
-// When the 32 lanes of a warp trace rays that share their x-y line (same
-// source, same detector column of a detector whose columns run along z: the
-// cone-beam and StaticCT rings), every x- and y-plane parameter is bitwise
-// the same for all lanes; only the z planes differ.  The per-lane merge walk
-// above then diverges at almost every step (some lane always takes a z step)
-// and the lanes drift apart along the x-y path.  Here the warp walks the x-y
-// cells together (warp-uniform state) and each lane splits a cell only at its
-// own z planes.  The segment end points are the same floats and they are
-// accumulated in the same order as in traverse(), so results are bitwise those
-// of the general walk; the gathers (forward) and reductions (adjoint) of a
-// warp now address one voxel column (i, j, k..k+~32) at a time.
-// A warp whose lanes do not share the x-y line falls back to traverse().
+// When the 32 lanes of a warp trace rays that share their x-y line (one
+// source, one detector column whose cells run along z: cone-beam views and
+// StaticCT rings tiled with 32 detector rows per warp), every x- and y-plane
+// parameter is bitwise the same for all lanes and only the z planes differ.
+// The per-lane walk then spends most of its compare / select work deriving
+// the same x-y crossings 32 times over.  Here the warp derives the merged x-y
+// crossing sequence once, 32 crossings per round: lane l evaluates the l-th
+// next x plane and the l-th next y plane, a rank search across the warp
+// places each in merged order, and the first 32 go to a per-warp shared
+// buffer together with the x-y column each one ends.  Every lane then walks
+// the buffer cell by cell (the same cell on all lanes, a broadcast read) and
+// splits the cell at its own next z plane when one falls inside it:
+//     te = min(t_cell_end, t_exit)      ts = min(t_next_z, te)
+//     segment A = [t_cur, ts] in (column, k)
+//     segment B = [ts, te]    in (column, k +- 1), empty unless a z plane lies inside
+// Segments are (t1 - t0) * |v| over the same plane parameters as the per-lane
+// walk, taken in the same order, and zero-length ones are skipped as there,
+// so the results are bitwise those of traverse<3, ADJ, false>.
+//
+// At most one z plane per cell: a cell spans at most the x or y plane
+// spacing in t, 1 / max(|v_x|, |v_y|), and z planes are 1 / |v_z| apart.  A
+// warp takes this walk only when every live lane has |v_z| <= 0.75 max(|v_x|,
+// |v_y|) and |s| <= 2^17 (with every grid dimension <= 2^16, checked on the
+// host), so |p - s| < 2^18 and float rounding of a plane parameter (< 2^-6 of
+// a spacing) cannot close the 25 % margin.  Other warps run the per-lane walk.
 // ----------------------------------------------------------------------------
 constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
+constexpr int kGroup = 4;   // cells walked per inner step (kChunk is a multiple)
 
+struct XYCell {
+    float t;  // parameter of the crossing that ends the cell
+    int col;  // flat index of the cell's (i, j) column at k = 0
+};
+
+// Per-lane set-up, the arithmetic of the start of traverse<3>.
 struct LaneRay {
-    float s[3], inv[3], ray_len, t_enter, t_exit;
+    float s[3], va[3], inv[3], ray_len, t_enter, t_exit;
     bool live;
 };
 
-// Per-lane set-up, identical arithmetic to the start of traverse<3>.
 __device__ __forceinline__ void lane_setup(LaneRay& R, const float* sw, const float* dw, const GridDims<3>& G,
-                                           const Affine3& A, int& fixed_idx, bool& z_parallel) {
-    float vw[3];
+                                           const Affine3& A) {
+    float vw[3], d[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
     R.ray_len = sqrtf(sumsq3(vw[0], vw[1], vw[2]));
     R.live = R.ray_len >= 1e-12f;
-    float d[3];
     world_to_index3(A, sw[0], sw[1], sw[2], R.s[0], R.s[1], R.s[2]);
     world_to_index3(A, dw[0], dw[1], dw[2], d[0], d[1], d[2]);
     R.t_enter = 0.f;
     R.t_exit = 1.f;
-    fixed_idx = 0;
-    z_parallel = false;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float va = __fsub_rn(d[a], R.s[a]);
         const float nf = (float)G.n[a];
+        R.va[a] = va;
         R.live = R.live && isfinite(R.s[a]) && isfinite(va);
         if (fabsf(va) > 1e-12f) {
             R.inv[a] = __frcp_rn(va);
@@ -331,20 +351,17 @@ __device__ __forceinline__ void lane_setup(LaneRay& R, const float* sw, const fl
             R.inv[a] = 0.f;
             const int i = __float2int_rn(R.s[a]);
             R.live = R.live && (i >= 0) && (i < G.n[a]);
-            fixed_idx += i * G.stride[a];
-            if (a == 2) z_parallel = true;
         }
     }
     R.live = R.live && (R.t_enter < R.t_exit);
 }
 
-// Slab index of a crossing axis at time t: behind-plane parameter <= t and
-// ahead-plane parameter > t (the fix-up of traverse), clamped into the grid.
-__device__ __forceinline__ int slab_at(float t, float s, float inv, int n) {
-    const float va_sign = inv;  // same sign as v
-    const float c = __fmaf_rn(t, __frcp_rn(inv), s);
-    int i = __float2int_rd(c + 0.5f);
-    if (va_sign > 0.f) {
+// Slab of a crossing axis at parameter t: behind-plane parameter <= t and
+// ahead-plane parameter > t, from an estimate fixed up with the exact plane
+// formula (the start rule of traverse), clamped into the grid.
+__device__ __forceinline__ int slab_at(float t, float s, float va, float inv, int n) {
+    int i = __float2int_rd(__fmaf_rn(t, va, s) + 0.5f);
+    if (va > 0.f) {
 #pragma unroll 1
         for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s, inv) <= t; ++k) ++i;
 #pragma unroll 1
@@ -358,13 +375,84 @@ __device__ __forceinline__ int slab_at(float t, float s, float inv, int n) {
     return min(max(i, 0), n - 1);
 }
 
-template <bool ADJ, bool MID>
-__global__ void __launch_bounds__(256) siddon3d_column_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                              const float* __restrict__ src,
-                                                              const float* __restrict__ dst, int64_t n_ray,
-                                                              const float* __restrict__ M_inv,
-                                                              const float* __restrict__ bvec, GridDims<3> G,
-                                                              int64_t nvox, Tiling T) {
+// Number of lanes m whose `sorted` value (non-decreasing over the lanes) is
+// below `key` (INCLUSIVE: at or below): a branch-free binary search.
+template <bool INCLUSIVE>
+__device__ __forceinline__ int warp_rank(float sorted, float key) {
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const float v = __shfl_sync(kFullMask, sorted, c + step - 1);
+        c += (INCLUSIVE ? v <= key : v < key) ? step : 0;
+    }
+    // c counts lanes 0..30; lane 31 is the one left to test
+    const float v = __shfl_sync(kFullMask, sorted, c);
+    return c + ((INCLUSIVE ? v <= key : v < key) ? 1 : 0);
+}
+
+// Per-lane z state of the shared x-y walk.
+struct ZWalk {
+    float t_cur, t_end, len, tnz, pnz, psz, s2, i2;
+    int kz, dsz;
+};
+
+// kGroup cells of the buffer from position q: segment A = [t_cur, ts] in
+// (column, k), segment B = [ts, te] in (column, k') after a z step.
+struct CellGroup {
+    float sa[kGroup], sb[kGroup];
+    unsigned ia[kGroup], ib[kGroup];  // voxel indices, valid where the segment is positive
+};
+
+__device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup& g, ZWalk& Z) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        const XYCell c = buf[q + u];
+        const float te = fminf(c.t, Z.t_end);
+        const float ts = fminf(Z.tnz, te);
+        g.sa[u] = __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len);
+        g.ia[u] = (unsigned)(c.col + Z.kz);
+        if (Z.tnz <= te) {  // a z plane inside the cell (or ending it)
+            Z.kz += Z.dsz;
+            Z.pnz += Z.psz;
+            Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
+        }
+        g.sb[u] = __fmul_rn(__fsub_rn(te, ts), Z.len);
+        g.ib[u] = (unsigned)(c.col + Z.kz);
+        Z.t_cur = fmaxf(Z.t_cur, te);
+    }
+}
+
+// A positive segment lies inside the lane's [t_enter, t_exit] and between
+// crossed planes only, so its voxel is inside the grid; zero-length ones
+// (before entry, after exit, ties) are neither read nor added.
+__device__ __forceinline__ void gather_group(const float* vol, const CellGroup& g, float* v, uint64_t pol) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        if (g.sa[u] > 0.f) v[u] = ld_keep(vol + g.ia[u], pol);
+        if (g.sb[u] > 0.f) v[kGroup + u] = ld_keep(vol + g.ib[u], pol);
+    }
+}
+
+__device__ __forceinline__ float accumulate_group(const CellGroup& g, const float* v, float acc) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        if (g.sa[u] > 0.f) acc = __fmaf_rn(v[u], g.sa[u], acc);
+        if (g.sb[u] > 0.f) acc = __fmaf_rn(v[kGroup + u], g.sb[u], acc);
+    }
+    return acc;
+}
+
+template <bool ADJ>
+__global__ void __launch_bounds__(256) siddon3d_shared_xy_kernel(const float* __restrict__ in,
+                                                                 float* __restrict__ out,
+                                                                 const float* __restrict__ src,
+                                                                 const float* __restrict__ dst, int64_t n_ray,
+                                                                 const float* __restrict__ M_inv,
+                                                                 const float* __restrict__ bvec, GridDims<3> G,
+                                                                 int64_t nvox, Tiling T) {
+    __shared__ XYCell cells[256 / 32][kChunk];
+    const int lane = threadIdx.x & 31;
+    XYCell* buf = cells[threadIdx.x >> 5];
     const int64_t r = tile_ray(T);
     const int64_t bi = blockIdx.y;
     const Affine3 A = load_affine3(M_inv, bvec);
@@ -372,168 +460,164 @@ __global__ void __launch_bounds__(256) siddon3d_column_kernel(const float* __res
     if (r >= 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            sw[a] = __ldg(src + r * 3 + a);
-            dw[a] = __ldg(dst + r * 3 + a);
+            sw[a] = ld_stream(src + r * 3 + a);
+            dw[a] = ld_stream(dst + r * 3 + a);
         }
     }
     float y = 0.f;
     if constexpr (ADJ) {
-        if (r >= 0) y = __ldg(in + bi * n_ray + r);
+        if (r >= 0) y = ld_stream(in + bi * n_ray + r);
     }
     LaneRay R;
-    int fixed_idx;
-    bool z_par;
-    lane_setup(R, sw, dw, G, A, fixed_idx, z_par);
+    lane_setup(R, sw, dw, G, A);
     R.live = R.live && (r >= 0) && (!ADJ || y != 0.f);
 
-    // Do the live lanes share their x-y line?  (Inactive lanes do not vote.)
     const unsigned live_mask = __ballot_sync(kFullMask, R.live);
     if (live_mask == 0u) {
-        if (!ADJ && r >= 0) out[bi * n_ray + r] = 0.f;
+        if (!ADJ && r >= 0) st_stream(out + bi * n_ray + r, 0.f);
         return;
     }
+    // Do the live lanes share their x-y line, and is every live lane's z
+    // slope inside the one-z-plane-per-cell bound?  (Dead lanes do not vote.)
     const int leader = __ffs(live_mask) - 1;
     const float s0 = __shfl_sync(kFullMask, R.s[0], leader), s1 = __shfl_sync(kFullMask, R.s[1], leader);
+    const float va0 = __shfl_sync(kFullMask, R.va[0], leader), va1 = __shfl_sync(kFullMask, R.va[1], leader);
     const float i0 = __shfl_sync(kFullMask, R.inv[0], leader), i1 = __shfl_sync(kFullMask, R.inv[1], leader);
-    const bool same = !R.live || (__float_as_uint(R.s[0]) == __float_as_uint(s0) &&
-                                  __float_as_uint(R.s[1]) == __float_as_uint(s1) &&
-                                  __float_as_uint(R.inv[0]) == __float_as_uint(i0) &&
-                                  __float_as_uint(R.inv[1]) == __float_as_uint(i1));
-    if (!__all_sync(kFullMask, same)) {
-        // lanes do not share the x-y line: per-lane merge walk
+    const float vxy = fmaxf(i0 != 0.f ? fabsf(va0) : 0.f, i1 != 0.f ? fabsf(va1) : 0.f);
+    const bool ok = !R.live || (__float_as_uint(R.s[0]) == __float_as_uint(s0) &&
+                                __float_as_uint(R.s[1]) == __float_as_uint(s1) &&
+                                __float_as_uint(R.va[0]) == __float_as_uint(va0) &&
+                                __float_as_uint(R.va[1]) == __float_as_uint(va1) &&
+                                fabsf(R.va[2]) <= 0.75f * vxy && fabsf(R.s[0]) <= 131072.f &&
+                                fabsf(R.s[1]) <= 131072.f && fabsf(R.s[2]) <= 131072.f);
+    if (!__all_sync(kFullMask, ok) || vxy == 0.f) {
         if (r < 0) return;
         if constexpr (ADJ) {
-            if (R.live) traverse<3, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
+            if (R.live) traverse<3, true, false>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
         } else {
-            out[bi * n_ray + r] =
-                R.live ? traverse<3, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox) : 0.f;
+            st_stream(out + bi * n_ray + r,
+                      R.live ? traverse<3, false, false>(in + bi * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
+                             : 0.f);
         }
         return;
     }
 
-    // ---- warp-uniform x-y walk (every lane holds the same values) ----------
-    const float nx = (float)G.n[0], ny = (float)G.n[1];
-    float txy_in = 0.f, txy_out = 1.f;
-    bool xy_ok = true;
-    int col = 0;  // flat index of the current (i, j) column, k = 0
-    float tnx = __int_as_float(0x7f800000), tny = tnx, pnx = 0.f, pny = 0.f, psx = 0.f, psy = 0.f;
-    int dsx = 0, dsy = 0;
-    if (i0 != 0.f) {
-        const bool pos = i0 > 0.f;
-        txy_in = fmaxf(txy_in, plane_t(pos ? -0.5f : nx - 0.5f, s0, i0));
-        txy_out = fminf(txy_out, plane_t(pos ? nx - 0.5f : -0.5f, s0, i0));
-    } else {
-        const int i = __float2int_rn(s0);
-        xy_ok = xy_ok && i >= 0 && i < G.n[0];
-        col += i * G.stride[0];
-    }
-    if (i1 != 0.f) {
-        const bool pos = i1 > 0.f;
-        txy_in = fmaxf(txy_in, plane_t(pos ? -0.5f : ny - 0.5f, s1, i1));
-        txy_out = fminf(txy_out, plane_t(pos ? ny - 0.5f : -0.5f, s1, i1));
-    } else {
-        const int j = __float2int_rn(s1);
-        xy_ok = xy_ok && j >= 0 && j < G.n[1];
-        col += j * G.stride[1];
-    }
-    // Every live lane's own interval [t_enter, t_exit] lies inside
-    // [txy_in, txy_out]; walk only the union of the lanes' intervals.
-    float te = R.live ? R.t_enter : __int_as_float(0x7f800000);
-    float tx = R.live ? R.t_exit : __int_as_float(0xff800000);
+    // ---- x-y start, warp-uniform: the slabs at the earliest lane entry ----
+    const float kInf = __int_as_float(0x7f800000);
+    float t_start = R.live ? R.t_enter : kInf, t_stop = R.live ? R.t_exit : -kInf;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        te = fminf(te, __shfl_xor_sync(kFullMask, te, o));
-        tx = fmaxf(tx, __shfl_xor_sync(kFullMask, tx, o));
+        t_start = fminf(t_start, __shfl_xor_sync(kFullMask, t_start, o));
+        t_stop = fmaxf(t_stop, __shfl_xor_sync(kFullMask, t_stop, o));
     }
-    txy_in = fmaxf(txy_in, te);
-    txy_out = fminf(txy_out, tx);
-    xy_ok = xy_ok && txy_in < txy_out;
+    int col = 0, dsx = 0, dsy = 0;
+    float pnx = 0.f, pny = 0.f, psx = 0.f, psy = 0.f;
     if (i0 != 0.f) {
-        const int i = slab_at(txy_in, s0, i0, G.n[0]);
-        col += i * G.stride[0];
-        psx = i0 > 0.f ? 1.f : -1.f;
-        dsx = i0 > 0.f ? G.stride[0] : -G.stride[0];
+        const int i = slab_at(t_start, s0, va0, i0, G.n[0]);
+        psx = va0 > 0.f ? 1.f : -1.f;
+        dsx = va0 > 0.f ? G.stride[0] : -G.stride[0];
         pnx = (float)i + 0.5f * psx;
-        tnx = plane_t(pnx, s0, i0);
+        col += i * G.stride[0];
+    } else {
+        col += __float2int_rn(s0) * G.stride[0];
     }
     if (i1 != 0.f) {
-        const int j = slab_at(txy_in, s1, i1, G.n[1]);
-        col += j * G.stride[1];
-        psy = i1 > 0.f ? 1.f : -1.f;
-        dsy = i1 > 0.f ? G.stride[1] : -G.stride[1];
+        const int j = slab_at(t_start, s1, va1, i1, G.n[1]);
+        psy = va1 > 0.f ? 1.f : -1.f;
+        dsy = va1 > 0.f ? G.stride[1] : -G.stride[1];
         pny = (float)j + 0.5f * psy;
-        tny = plane_t(pny, s1, i1);
+        col += j * G.stride[1];
+    } else {
+        col += __float2int_rn(s1) * G.stride[1];
     }
 
-    // ---- per-lane z state, started at the lane's own entry ----------------
-    float tnz = __int_as_float(0x7f800000), pnz = 0.f, psz = 0.f;
-    int kz = 0, dsz = 0;
+    // ---- per-lane z state at the lane's own entry ------------------------
+    // Dead lanes keep t_cur = t_end = 0 and no z plane: every segment they
+    // form has zero length.
+    ZWalk Z;
+    Z.s2 = R.s[2];
+    Z.i2 = R.inv[2];
+    Z.t_cur = 0.f;
+    Z.t_end = 0.f;
+    Z.len = 0.f;
+    Z.tnz = kInf;
+    Z.pnz = 0.f;
+    Z.psz = 0.f;
+    Z.kz = 0;
+    Z.dsz = 0;
     if (R.live) {
-        if (!z_par) {
-            const int k = slab_at(R.t_enter, R.s[2], R.inv[2], G.n[2]);
-            kz = k * G.stride[2];
-            psz = R.inv[2] > 0.f ? 1.f : -1.f;
-            dsz = R.inv[2] > 0.f ? G.stride[2] : -G.stride[2];
-            pnz = (float)k + 0.5f * psz;
-            tnz = plane_t(pnz, R.s[2], R.inv[2]);
+        Z.t_cur = R.t_enter;
+        Z.t_end = R.t_exit;
+        Z.len = R.ray_len;
+        if (Z.i2 != 0.f) {
+            const int k = slab_at(Z.t_cur, Z.s2, R.va[2], Z.i2, G.n[2]);
+            Z.psz = R.va[2] > 0.f ? 1.f : -1.f;
+            Z.dsz = R.va[2] > 0.f ? G.stride[2] : -G.stride[2];
+            Z.pnz = (float)k + 0.5f * Z.psz;
+            Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
+            Z.kz = k * G.stride[2];
         } else {
-            kz = fixed_idx - (fixed_idx / G.stride[1]) * G.stride[1];  // the k part of the fixed index
+            Z.kz = __float2int_rn(Z.s2) * G.stride[2];
         }
     }
-    const float* vol = in + bi * nvox;
-    float* vout = out + bi * nvox;
+
+    // ---- rounds of 32 x-y crossings ---------------------------------------
+    // Each round consumes 32 crossings of the x-y sequence; after
+    // n_x + n_y + 2 of them both exit planes lie behind, so the bound below
+    // is never the reason the loop ends.
+    const float* __restrict__ vol = ADJ ? nullptr : pin_ptr(in + bi * nvox);
+    float* __restrict__ vout = ADJ ? pin_ptr(out + bi * nvox) : nullptr;
     float acc = 0.f;
-    const int max_xy = G.n[0] + G.n[1] + 3;
-    const int max_z = G.n[2] + 3;
-    int zsteps = 0;
-    float ta = txy_in;
+    const uint64_t pol = l2_policy_keep();
+    const float fl = (float)lane;
+    const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
 #pragma unroll 1
-    for (int it = 0; it < max_xy && xy_ok; ++it) {
-        const float tm = fminf(tnx, tny);
-        const bool last = !(tm < txy_out);
-        const float tb = last ? txy_out : tm;
-        if (R.live) {
-            float t0 = fmaxf(ta, R.t_enter);
-            const float tend = fminf(tb, R.t_exit);
+    for (int round = 0; round < max_rounds; ++round) {
+        // lane l: the l-th next x plane and the l-th next y plane (plane
+        // coordinates are exact: |p| < 2^17 in steps of 1)
+        const float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
+        const float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
+        // merged positions; on equal parameters the x crossing comes first
+        const int rx = lane + warp_rank<false>(ty, tx);
+        const int ry = lane + warp_rank<true>(tx, ty);
+        if (rx < kChunk) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
+        if (ry < kChunk) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
+        const int n_x = __popc(__ballot_sync(kFullMask, rx < kChunk));
+        __syncwarp();
+        // cells up to and including the one that ends at or after t_stop
+        const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
+        const int n_cells = min(n_in + 1, kChunk);
+        if constexpr (ADJ) {
 #pragma unroll 1
-            while (t0 < tend && zsteps < max_z) {
-                if (tnz <= t0) {  // a z plane at or before t0 has been crossed
-                    kz += dsz;
-                    pnz += psz;
-                    tnz = plane_t(pnz, R.s[2], R.inv[2]);
-                    ++zsteps;
-                    continue;
-                }
-                const float t1 = fminf(tend, tnz);
-                int idx = col + kz;
-                if constexpr (MID) {
-                    float vw[3];
+            for (int q = 0; q < n_cells; q += kGroup) {
+                CellGroup g;
+                walk_group(buf, q, g, Z);
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
-                    idx = midpoint_voxel<3>(A, sw, vw, t0, t1, G);
+                for (int u = 0; u < kGroup; ++u) {
+                    red_add_if(vout + g.ia[u], __fmul_rn(y, g.sa[u]), g.sa[u] > 0.f);
+                    red_add_if(vout + g.ib[u], __fmul_rn(y, g.sb[u]), g.sb[u] > 0.f);
                 }
-                if ((unsigned)idx < (unsigned)nvox) {
-                    const float seg = __fmul_rn(__fsub_rn(t1, t0), R.ray_len);
-                    if constexpr (ADJ) atomicAdd(vout + idx, __fmul_rn(y, seg));
-                    else acc = __fmaf_rn(__ldg(vol + idx), seg, acc);
-                }
-                t0 = t1;
+            }
+        } else {
+            // the group's gathers are issued together (up to 2 * kGroup in
+            // flight), then accumulated in walk order
+#pragma unroll 1
+            for (int q = 0; q < n_cells; q += kGroup) {
+                CellGroup g;
+                float v[2 * kGroup];
+                walk_group(buf, q, g, Z);
+                gather_group(vol, g, v, pol);
+                acc = accumulate_group(g, v, acc);
             }
         }
-        if (last) break;
-        ta = tb;
-        if (tnx == tm) {
-            col += dsx;
-            pnx += psx;
-            tnx = plane_t(pnx, s0, i0);
-        } else {
-            col += dsy;
-            pny += psy;
-            tny = plane_t(pny, s1, i1);
-        }
+        if (n_in < kChunk) break;
+        __syncwarp();  // every lane is done with this round's cells
+        col += n_x * dsx + (kChunk - n_x) * dsy;
+        pnx = __fmaf_rn((float)n_x, psx, pnx);
+        pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
     }
     if constexpr (!ADJ) {
-        if (r >= 0) out[bi * n_ray + r] = acc;
+        if (r >= 0) st_stream(out + bi * n_ray + r, acc);
     }
 }
 
@@ -582,16 +666,13 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     const bool flat = tiling == nullptr || tiling->n_view == 0;
     const int walk = tiling == nullptr ? CTLAB_WALK_AUTO : tiling->walk;
     if constexpr (NDIM == 3) {
-        // Detector-row tilings (a warp = 32 rows of one column) may take the
-        // column-coherent walk; it checks per warp that the lanes share their
-        // x-y line and otherwise runs the per-lane walk.
-        if (!flat && T.tile_rows % 32 == 0 && walk == CTLAB_WALK_COLUMN) {
-            if (mid)
-                siddon3d_column_kernel<ADJ, true>
-                    <<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
-            else
-                siddon3d_column_kernel<ADJ, false>
-                    <<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+        // Detector-row tilings (a warp = 32 rows of one column) under the
+        // crossing rule take the shared x-y walk; it checks per warp that the
+        // lanes share their x-y line and otherwise runs the per-lane walk.
+        const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
+        if (!flat && !mid && small_grid && T.tile_rows % 32 == 0 &&
+            (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
+            siddon3d_shared_xy_kernel<ADJ><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
             return launch_status(what);
         }
     }

@@ -81,10 +81,15 @@ int ctlab_invert_matrix(const float* M, int n, float* M_inv, int* singular, void
  */
 #define CTLAB_VOXEL_MIDPOINT 0
 #define CTLAB_VOXEL_CROSSING 1
-/* Walk: CTLAB_WALK_LANE walks each ray on its own lane; CTLAB_WALK_COLUMN
- * (3-D, detector-row tilings with tile_rows a multiple of 32) walks the x-y
- * cells of a warp's shared line once and splits them per lane at z planes;
- * CTLAB_WALK_AUTO picks the faster measured one (currently the lane walk). */
+/* Walk: CTLAB_WALK_LANE walks each ray on its own lane.  CTLAB_WALK_COLUMN
+ * (3-D, crossing rule, detector-row tilings with tile_rows a multiple of 32,
+ * grid dimensions <= 65536) derives the merged x-y crossings of a warp's
+ * shared line once per warp and splits each x-y cell per lane at its z
+ * planes; warps whose rays do not share their x-y line, or whose z slope is
+ * steeper than 3/4 of the x-y slope, fall back to the lane walk inside the
+ * same launch.  Both give bitwise equal forward projections.
+ * CTLAB_WALK_AUTO takes the column walk wherever it applies (it is the
+ * faster one measured) and the lane walk elsewhere. */
 #define CTLAB_WALK_AUTO 0
 #define CTLAB_WALK_LANE 1
 #define CTLAB_WALK_COLUMN 2
