@@ -1,7 +1,7 @@
 """ctypes binding of libctlab_b200.so (the C ABI declared in include/ctlab_b200.h).
 
 The library is required: importing this module raises ImportError when it
-has not been built (``python -m ct_laboratory_b200.build``).  There is no
+has not been built (``python ct_laboratory_b200/build.py``).  There is no
 Python or CPU fallback for any projector.
 """
 from __future__ import annotations
@@ -16,7 +16,7 @@ _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "li
 if not os.path.exists(_LIB_PATH):
     raise ImportError(
         f"ct_laboratory_b200: native library {_LIB_PATH} is missing; build it with "
-        "`python -m ct_laboratory_b200.build` (nvcc, sm_100a)")
+        "`python ct_laboratory_b200/build.py` (nvcc, sm_100a)")
 
 lib = ctypes.CDLL(_LIB_PATH)
 
@@ -40,6 +40,27 @@ class RayOpts(ctypes.Structure):
 
 
 _TP = ctypes.POINTER(RayOpts)
+
+
+class Scan(ctypes.Structure):
+    """Mirror of ctlab_scan (include/ctlab_b200.h): one scan of a batch."""
+
+    _fields_ = [("image_in", _P), ("sino_out", _P), ("sino_in", _P), ("image_out", _P), ("src", _P), ("dst", _P),
+                ("M_inv", _P), ("b", _P), ("n_ray", _I64), ("dims", _I64 * 3), ("ndim", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("opts", RayOpts)]
+
+
+class Batch(ctypes.Structure):
+    """Mirror of ctlab_batch (include/ctlab_b200.h): a plan of a batch."""
+
+    _fields_ = [("workspace", _P), ("total_tiles", _I64), ("n_scan", ctypes.c_int32), ("ndim", ctypes.c_int32),
+                ("block_threads", ctypes.c_int32), ("voxel_rule", ctypes.c_int32), ("has_forward", ctypes.c_int32),
+                ("has_adjoint", ctypes.c_int32), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+_SP = ctypes.POINTER(Scan)
+_BP = ctypes.POINTER(Batch)
+_I32 = ctypes.c_int32
 
 # name -> argtypes (every entry point returns int)
 _SIGS = {
@@ -65,6 +86,10 @@ _SIGS = {
     "ctlab_back_project_2d_siddon": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P],
     "ctlab_invert_matrix": [_P, _I, _P, _P, _P],
     "ctlab_back_project_3d_gather": [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I64, _P, _P],
+    "ctlab_batch_plan": [_SP, _I32, _I32, _P, _I64, _BP, _P],
+    "ctlab_forward_project_batched": [_BP, _I32, _P],
+    "ctlab_back_project_batched": [_BP, _I, _I32, _P],
+    "ctlab_batch_default_ctas": [_I32, _I, _I, _I32, ctypes.POINTER(_I32)],
 }
 
 for _name, _args in _SIGS.items():
@@ -76,13 +101,15 @@ lib.ctlab_last_error.restype = ctypes.c_char_p
 lib.ctlab_last_error.argtypes = []
 lib.ctlab_abi_version.restype = ctypes.c_int
 lib.ctlab_abi_version.argtypes = []
+lib.ctlab_batch_workspace_bytes.restype = ctypes.c_int64
+lib.ctlab_batch_workspace_bytes.argtypes = [_I32]
 
 ABI_VERSION = lib.ctlab_abi_version()
 
 
 def exported_symbols():
     """Names of the C entry points this binding declares."""
-    return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version"]
+    return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version", "ctlab_batch_workspace_bytes"]
 
 
 def call(name: str, *args) -> None:

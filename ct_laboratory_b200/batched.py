@@ -1,0 +1,317 @@
+"""Many scans projected in one persistent launch, with an autotuner and
+CUDA-graph replay.
+
+``ScanBatch(projectors)`` binds a list of 2-D projectors
+(``CTProjector2DModule`` and its fan-beam / StaticCT subclasses) or of 3-D
+projectors (``CTProjector3DModule`` and subclasses) to device buffers it
+allocates once:
+
+  images_in[i]   forward input of scan i          ([n_row, n_col] or [n_x, n_y, n_z])
+  sinos_out[i]   forward output                   ([n_ray])
+  sinos_in[i]    adjoint input                    ([n_ray])
+  images_out[i]  adjoint output                   (same shape as images_in[i])
+
+``forward()`` computes every sinos_out[i] = A_i images_in[i] in one launch
+of persistent CTAs that pull ray tiles of all scans from a device work
+counter (libctlab_b200.so ``ctlab_forward_project_batched``); ``back()`` the
+adjoints likewise.  ``forward_loop()`` / ``back_loop()`` run the very same
+walks one scan at a time through the single-scan entry points, into the
+same buffers: the per-instance loop the batch replaces.  Forward results are
+bitwise equal between the two; adjoints up to the order of float atomics.
+
+Tile shapes (rays per CTA and how they are laid over each scan's detector)
+are chosen by ``autotune()``, which times the candidates on the batch itself
+and caches the winner per batch signature.  ``capture()`` records forward
+and / or adjoint into a ``torch.cuda.CUDAGraph`` for replay.
+
+The reference has no batched launch: its projector modules take one scan
+per call (tomography/ct_projector_3d_module.py:171-188,
+ct_projector_2d_module.py:50-65).
+"""
+from __future__ import annotations
+
+import ctypes
+import statistics
+
+import torch
+
+from . import _native as N
+from .tomography.ct_projector_3d_module import CTProjector3DModule
+
+__all__ = ["ScanBatch", "Autotuner", "tile_kinds"]
+
+
+def _ndim(p):
+    return 3 if isinstance(p, CTProjector3DModule) else 2
+
+
+def _dims(p):
+    return (p.n_x, p.n_y, p.n_z) if _ndim(p) == 3 else (p.n_row, p.n_col)
+
+
+def _ray_grid(p):
+    """(n_view, n_bin) when the projector's rays are ordered [view][bin] with
+    n_bin detector cells per view, else None."""
+    n_ray = int(p.src.shape[0])
+    if hasattr(p, "n_view") and hasattr(p, "n_det"):  # fan-beam: [view][cell]
+        bins = int(p.n_det)
+    elif hasattr(p, "n_module") and hasattr(p, "det_n_col"):  # uniform StaticCT ring: [source][module][col]
+        bins = int(p.n_module) * int(p.det_n_col)
+    else:
+        return None
+    if bins <= 0 or n_ray % bins:
+        return None
+    return n_ray // bins, bins
+
+
+def tile_kinds(p):
+    """Tile layouts that apply to projector p (the autotuner's choices).
+
+    flat      consecutive rays, block_threads per CTA
+    grid32    2-D: 32 detector cells x (block_threads/32) views per CTA
+    grid64    2-D: 64 cells x (block_threads/64) views
+    col32     3-D detector grid: 32 detector rows x (block_threads/32) columns
+              (lanes of a warp down one detector column: the column walk)
+    col64     3-D: 64 rows x (block_threads/64) columns
+    """
+    kinds = ["flat"]
+    if _ndim(p) == 2:
+        if _ray_grid(p) is not None:
+            kinds += ["grid32", "grid64"]
+    elif getattr(p, "ray_tiling", None) is not None and p.ray_tiling.n_view > 0:
+        kinds += ["col32", "col64"]
+    return kinds
+
+
+def _opts(p, kind, voxel_rule, block_threads):
+    """RayOpts of projector p laid out as `kind` (falls back to flat when the
+    kind does not apply or does not fit block_threads)."""
+    rows = {"grid32": 32, "grid64": 64, "col32": 32, "col64": 64}.get(kind)
+    if rows is None or rows > block_threads or kind not in tile_kinds(p):
+        return N.flat_opts(voxel_rule=voxel_rule, block_threads=block_threads)
+    if kind.startswith("grid"):
+        n_view, n_bin = _ray_grid(p)
+        # rows = detector cells (stride 1), columns = views (stride n_bin)
+        return N.tiling(1, n_bin, n_view, n_bin * n_view, 1, n_bin, tile_rows=rows, block_threads=block_threads,
+                        voxel_rule=voxel_rule)
+    t = p.ray_tiling
+    return N.tiling(t.n_view, t.n_row, t.n_col, t.view_stride, t.row_stride, t.col_stride, tile_rows=rows,
+                    block_threads=block_threads, voxel_rule=voxel_rule)
+
+
+def _cost(p):
+    """Rough cost of one ray of p (planes it may cross): heavy scans go first."""
+    return sum(_dims(p))
+
+
+class ScanBatch:
+    def __init__(self, projectors, voxel_rule=N.VOXEL_CROSSING, forward=True, adjoint=True, block_threads=256,
+                 kind="auto"):
+        self.projectors = list(projectors)
+        if not self.projectors:
+            raise ValueError("ScanBatch needs at least one projector")
+        nd = {_ndim(p) for p in self.projectors}
+        if len(nd) != 1:
+            raise ValueError("ScanBatch: all projectors must be 2-D or all 3-D")
+        self.ndim = nd.pop()
+        self.device = self.projectors[0].src.device
+        if self.device.type != "cuda":
+            raise RuntimeError("ScanBatch: projectors must live on a CUDA device (there is no CPU implementation)")
+        self.voxel_rule = int(voxel_rule)
+        self.has_forward, self.has_adjoint = bool(forward), bool(adjoint)
+        shapes = [_dims(p) for p in self.projectors]
+        n_rays = [int(p.src.shape[0]) for p in self.projectors]
+        self.images_in = self._arena(shapes) if forward else None
+        self.sinos_out = self._arena([(n,) for n in n_rays]) if forward else None
+        self.sinos_in = self._arena([(n,) for n in n_rays]) if adjoint else None
+        self.images_out = self._arena(shapes) if adjoint else None
+        # heaviest rays first: long tiles start early, short ones fill the tail
+        self.order = sorted(range(len(self.projectors)), key=lambda i: -_cost(self.projectors[i]))
+        nbytes = N.lib.ctlab_batch_workspace_bytes(len(self.projectors))
+        if nbytes < 0:
+            raise ValueError(f"ScanBatch: {len(self.projectors)} scans is outside [1, 65535]")
+        self._ws = torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=self.device)
+        off = (-self._ws.data_ptr()) % 256
+        self._ws_ptr = self._ws.data_ptr() + off
+        self._ws_bytes = int(nbytes)
+        self._plan = N.Batch()
+        self.config = None
+        self.configure(block_threads=block_threads, kind=kind)
+
+    # ------------------------------------------------------------ buffers
+    def _arena(self, shapes):
+        """One allocation holding a zeroed tensor per shape, each 256-byte aligned."""
+        sizes = [int(torch.Size(s).numel()) for s in shapes]
+        pad = lambda n: (n + 63) // 64 * 64  # noqa: E731  (64 floats = 256 bytes)
+        total = sum(pad(n) for n in sizes)
+        flat = torch.zeros(max(total, 1), dtype=torch.float32, device=self.device)
+        out, off = [], 0
+        for s, n in zip(shapes, sizes):
+            out.append(flat[off:off + n].view(s))
+            off += pad(n)
+        return out
+
+    # ------------------------------------------------------------ planning
+    def _scan(self, i, kind, block_threads):
+        p = self.projectors[i]
+        s = N.Scan()
+        if self.has_forward:
+            s.image_in, s.sino_out = self.images_in[i].data_ptr(), self.sinos_out[i].data_ptr()
+        if self.has_adjoint:
+            s.sino_in, s.image_out = self.sinos_in[i].data_ptr(), self.images_out[i].data_ptr()
+        s.src, s.dst = p.src.data_ptr(), p.dst.data_ptr()
+        s.M_inv, s.b = p.M_inv.data_ptr(), p.b.data_ptr()
+        s.n_ray = int(p.src.shape[0])
+        d = _dims(p)
+        for a in range(3):
+            s.dims[a] = int(d[a]) if a < len(d) else 0
+        s.ndim = self.ndim
+        k = kind if isinstance(kind, str) else kind[i]
+        s.opts = _opts(p, k, self.voxel_rule, block_threads)
+        return s
+
+    def configure(self, block_threads=256, kind="auto", n_cta=0):
+        """(Re)plan the batch with a tile layout: `kind` is one tile kind for
+        every scan (the first that applies when it is "auto": col32 / grid32 /
+        flat) or a list with one kind per scan."""
+        if kind == "auto":
+            kind = ["col32" if "col32" in tile_kinds(p) else "flat" for p in self.projectors]
+        arr = (N.Scan * len(self.projectors))(*[self._scan(i, kind, block_threads) for i in self.order])
+        with torch.cuda.device(self.device):
+            N.call("ctlab_batch_plan", arr, len(self.projectors), int(block_threads), ctypes.c_void_p(self._ws_ptr),
+                   self._ws_bytes, ctypes.byref(self._plan), N.stream_of(self._ws))
+            if n_cta == 0:
+                v = ctypes.c_int32(0)
+                N.call("ctlab_batch_default_ctas", self.ndim, int(self.has_adjoint and not self.has_forward),
+                       self.voxel_rule, int(block_threads), ctypes.byref(v))
+                n_cta = v.value
+        self.config = {"block_threads": int(block_threads), "kind": kind, "n_cta": int(n_cta)}
+        self._loop_opts = [_opts(self.projectors[i], kind if isinstance(kind, str) else kind[i], self.voxel_rule,
+                                 block_threads) for i in range(len(self.projectors))]
+        return self.config
+
+    @property
+    def total_tiles(self):
+        return int(self._plan.total_tiles)
+
+    # ------------------------------------------------------------ launches
+    def forward(self):
+        """sinos_out[i] = A_i images_in[i] for every scan, one launch."""
+        with torch.cuda.device(self.device):
+            N.call("ctlab_forward_project_batched", ctypes.byref(self._plan), self.config["n_cta"],
+                   N.stream_of(self._ws))
+
+    def back(self, accumulate=False):
+        """images_out[i] (+)= A_i^T sinos_in[i] for every scan: one zeroing
+        launch (unless accumulating) and one persistent launch."""
+        with torch.cuda.device(self.device):
+            N.call("ctlab_back_project_batched", ctypes.byref(self._plan), int(bool(accumulate)),
+                   self.config["n_cta"], N.stream_of(self._ws))
+
+    def forward_loop(self):
+        """The same forward one scan at a time (single-scan entry points)."""
+        st = N.stream_of(self._ws)
+        with torch.cuda.device(self.device):
+            for i, p in enumerate(self.projectors):
+                o = self._loop_opts[i]
+                if self.ndim == 3:
+                    N.call("ctlab_forward_project_3d_on_the_fly_ex", N.ptr(self.images_in[i]), 1, p.n_x, p.n_y,
+                           p.n_z, N.ptr(p.src), N.ptr(p.dst), int(p.src.shape[0]), N.ptr(p.M_inv), N.ptr(p.b),
+                           N.ptr(self.sinos_out[i]), ctypes.byref(o), st)
+                else:
+                    N.call("ctlab_forward_project_2d_siddon", N.ptr(self.images_in[i]), 1, p.n_row, p.n_col,
+                           N.ptr(p.src), N.ptr(p.dst), int(p.src.shape[0]), N.ptr(p.M_inv), N.ptr(p.b),
+                           N.ptr(self.sinos_out[i]), ctypes.byref(o), st)
+
+    def back_loop(self, accumulate=False):
+        """The same adjoint one scan at a time (single-scan entry points)."""
+        st = N.stream_of(self._ws)
+        acc = int(bool(accumulate))
+        with torch.cuda.device(self.device):
+            for i, p in enumerate(self.projectors):
+                o = self._loop_opts[i]
+                if self.ndim == 3:
+                    N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
+                           N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), st)
+                else:
+                    N.call("ctlab_back_project_2d_siddon", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
+                           N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_row, p.n_col,
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), st)
+
+    def capture(self, forward=True, adjoint=True, accumulate=False):
+        """A CUDA graph of one forward and / or adjoint pass of the batch
+        (replay with .replay(); the bound buffers must stay in place)."""
+        with torch.cuda.device(self.device):
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(side):  # warm-up outside the capture
+                if forward:
+                    self.forward()
+                if adjoint:
+                    self.back(accumulate)
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                if forward:
+                    self.forward()
+                if adjoint:
+                    self.back(accumulate)
+        return g
+
+    def autotune(self, reps=3, block_threads=(128, 256), tuner=None):
+        """Pick the fastest (block_threads, tile kind) for this batch by timing
+        forward + adjoint passes; the result is cached per batch signature."""
+        return (tuner or DEFAULT_TUNER).tune(self, reps=reps, block_threads=block_threads)
+
+    def signature(self):
+        return (self.ndim, self.voxel_rule, self.has_forward, self.has_adjoint,
+                tuple((_dims(p), int(p.src.shape[0]), tuple(tile_kinds(p))) for p in self.projectors))
+
+
+class Autotuner:
+    """Times every candidate launch shape of a batch with CUDA events (median
+    of `reps` forward + adjoint passes after one warm-up) and keeps the
+    fastest per batch signature."""
+
+    def __init__(self):
+        self.cache = {}
+        self.trials = {}
+
+    def candidates(self, batch, block_threads):
+        kinds = sorted({k for p in batch.projectors for k in tile_kinds(p)})
+        return [(bt, k) for bt in block_threads for k in kinds]
+
+    def _time(self, batch, reps):
+        def one():
+            if batch.has_forward:
+                batch.forward()
+            if batch.has_adjoint:
+                batch.back()
+        one()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            one()
+            e1.record()
+            torch.cuda.synchronize(batch.device)
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def tune(self, batch, reps=3, block_threads=(128, 256)):
+        key = batch.signature()
+        if key not in self.cache:
+            results = []
+            with torch.cuda.device(batch.device):
+                for bt, kind in self.candidates(batch, block_threads):
+                    batch.configure(block_threads=bt, kind=kind)
+                    results.append((self._time(batch, reps), bt, kind))
+            results.sort()
+            self.trials[key] = results
+            self.cache[key] = {"block_threads": results[0][1], "kind": results[0][2]}
+        best = self.cache[key]
+        return batch.configure(block_threads=best["block_threads"], kind=best["kind"])
+
+
+DEFAULT_TUNER = Autotuner()

@@ -1,6 +1,7 @@
 """Build libctlab_b200.so (the C-ABI library) in-tree with nvcc for sm_100a.
 
-    python -m ct_laboratory_b200.build          # or: python ct_laboratory_b200/build.py
+    python ct_laboratory_b200/build.py [--force]   # (not -m: that would import the package,
+                                                   #  which needs the library already built)
 
 The library lands in ct_laboratory_b200/_lib/ next to the package so that it
 travels with the source tree; the loader (ct_laboratory_b200/_native.py)
@@ -20,7 +21,7 @@ LIB_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIB_DIR, "libctlab_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["capi.cu", "siddon.cu", "tvals.cu", "gather.cu"]
+SOURCES = ["capi.cu", "siddon.cu", "tvals.cu", "gather.cu", "batched.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,364 @@
+// batched.cu — many scans in one persistent launch (sm_100a).
+//
+// A reconstruction service or a study with many small scans calls the
+// projector once per scan: dozens of launches of a few hundred CTAs each,
+// most of them too small to fill 148 SMs, each paying launch latency and a
+// tail where the GPU drains.  Here the scans of a batch (uneven image sizes,
+// view counts and geometries: fan-beam views, StaticCT rings, cone-beam
+// scans) are cut into ray tiles, laid end to end, and one launch of
+// persistent CTAs (resident CTAs per SM x SMs) pulls tiles from a device work
+// counter until the batch is done.  Scans are listed heaviest first by the
+// caller (the Python planner orders them), so the long tiles start early and
+// the short ones fill the tail.
+//
+// Every tile is walked by the same device code as the single-scan kernels
+// (walk.cuh): 2-D scans by the per-lane walk, 3-D crossing-rule scans by the
+// shared x-y column walk (which falls back to the per-lane walk in warps
+// whose rays do not share their x-y line), midpoint-rule scans by the
+// per-lane midpoint walk.  Results are therefore those of the single-scan
+// entry points: bitwise for the forward; for the adjoint up to the order of
+// the float atomic additions.
+//
+// Scratch: a plan's workspace (device memory the caller allocates, size from
+// ctlab_batch_workspace_bytes) holds the work counter and the scan
+// descriptor table.  ctlab_batch_plan validates the scans on the host and
+// copies the table in once; the launch entry points then only reset the
+// counter (cudaMemsetAsync) and launch, so they can be replayed from a CUDA
+// graph as long as the bound buffers stay where they are.
+#include "walk.cuh"
+
+#include <vector>
+
+namespace ctlab {
+
+// Resolved scan descriptor as the kernels read it.
+struct ScanDev {
+    const float* image_in;
+    float* sino_out;
+    const float* sino_in;
+    float* image_out;
+    const float* src;
+    const float* dst;
+    const float* M_inv;
+    const float* b;
+    int64_t n_ray;
+    int64_t nvox;
+    Tiling T;
+    int64_t first_tile;  // first tile of this scan in the batch
+    int n[3], stride[3];
+};
+
+struct BatchHeader {
+    unsigned counter;  // next tile to hand out
+    unsigned pad[63];  // keeps the descriptor table 256-byte aligned
+};
+static_assert(sizeof(BatchHeader) == 256, "header must be 256 bytes");
+
+constexpr int64_t kMaxBatchScans = 65535;        // grid.y of the zeroing kernel
+constexpr int64_t kMaxBatchTiles = 1LL << 31;    // the work counter is 32-bit
+
+static int64_t table_bytes(int64_t n_scan) {
+    return ((n_scan * (int64_t)sizeof(ScanDev) + 255) / 256) * 256;
+}
+
+// Scan index of tile t: the last scan whose first tile is <= t (scans with
+// no tiles share their first tile with the next one and are skipped).
+__device__ __forceinline__ int find_scan(const ScanDev* __restrict__ scans, int n_scan, unsigned t) {
+    int lo = 0, hi = n_scan - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((unsigned)__ldg(&scans[mid].first_tile) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Resident CTAs per SM the register allocation of the batched kernels targets.
+#ifndef CTLAB_BATCH_MIN_BLOCKS
+#define CTLAB_BATCH_MIN_BLOCKS 4
+#endif
+
+// One persistent CTA: take a tile, walk its rays, repeat.  MID selects the
+// midpoint voxel rule for every scan of the batch.  Thread 0 takes the next
+// tile and the whole CTA works on it, so the warp-collective steps of the
+// column walk always see full warps.
+template <int NDIM, bool ADJ, bool MID>
+__global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
+    batched_kernel(const ScanDev* __restrict__ scans, int n_scan, unsigned total_tiles, unsigned* __restrict__ counter) {
+    __shared__ XYCell cells[256 / 32][kChunk];
+    __shared__ unsigned s_tile;
+    __shared__ int s_scan;
+    XYCell* buf = cells[threadIdx.x >> 5];
+#pragma unroll 1
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(counter, 1u);
+            s_tile = t;
+            s_scan = t < total_tiles ? find_scan(scans, n_scan, t) : 0;
+        }
+        __syncthreads();
+        const unsigned t = s_tile;
+        const int si = s_scan;
+        __syncthreads();  // s_tile / s_scan may be overwritten from here on
+        if (t >= total_tiles) return;
+        const ScanDev* S = scans + si;
+        Tiling T;
+        T.n_view = S->T.n_view;
+        T.n_row = S->T.n_row;
+        T.n_col = S->T.n_col;
+        T.view_stride = S->T.view_stride;
+        T.row_stride = S->T.row_stride;
+        T.col_stride = S->T.col_stride;
+        T.tile_rows = S->T.tile_rows;
+        T.tile_cols = S->T.tile_cols;
+        T.tiles_r = S->T.tiles_r;
+        T.tiles_c = S->T.tiles_c;
+        T.n_blocks = S->T.n_blocks;
+        const int64_t r = tile_ray_at(T, t - (unsigned)S->first_tile);
+        const float* in = ADJ ? S->sino_in : S->image_in;
+        float* out = ADJ ? S->image_out : S->sino_out;
+        const int64_t n_ray = S->n_ray, nvox = S->nvox;
+        GridDims<NDIM> G;
+#pragma unroll
+        for (int a = 0; a < NDIM; ++a) {
+            G.n[a] = S->n[a];
+            G.stride[a] = S->stride[a];
+        }
+        if constexpr (NDIM == 3) {
+            const Affine3 A = load_affine3(S->M_inv, S->b);
+            if constexpr (MID) {
+                if (r >= 0) lane_ray<3, ADJ, true>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            } else {
+                shared_xy_ray<ADJ>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0, buf);
+            }
+        } else {
+            const Affine2 A = load_affine2(S->M_inv, S->b);
+            if (r >= 0) lane_ray<2, ADJ, MID>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+        }
+    }
+}
+
+// Zeroes every scan's image_out: blockIdx.y = scan, grid-stride in float4
+// where the buffer is 16-byte aligned.
+__global__ void batched_zero_kernel(const ScanDev* __restrict__ scans) {
+    const ScanDev* S = scans + blockIdx.y;
+    float* p = S->image_out;
+    const int64_t n = S->nvox;
+    if (p == nullptr) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+        float4* q = reinterpret_cast<float4*>(p);
+        const int64_t n4 = n >> 2;
+        for (int64_t i = i0; i < n4; i += stride) q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int64_t i = (n4 << 2) + i0; i < n; i += stride) p[i] = 0.f;
+    } else {
+        for (int64_t i = i0; i < n; i += stride) p[i] = 0.f;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// host side
+// ----------------------------------------------------------------------------
+
+// Validates one scan and resolves it into `D`; `what` names it in messages.
+static int resolve_scan(const ctlab_scan& s, int64_t idx, int ndim, int block_threads, int voxel_rule, ScanDev& D) {
+    CTLAB_REQUIRE(s.ndim == ndim, "batch: scan %lld has ndim %d, the batch's first scan has %d", (long long)idx,
+                  s.ndim, ndim);
+    CTLAB_REQUIRE(s.n_ray >= 0, "batch: scan %lld has n_ray < 0", (long long)idx);
+    int64_t nvox = 1;
+    for (int a = 0; a < ndim; ++a) {
+        const int64_t lim = ndim == 3 ? 65536 : (1 << 22);
+        CTLAB_REQUIRE(s.dims[a] >= 1 && s.dims[a] <= lim, "batch: scan %lld grid dimension %d out of range (%lld)",
+                      (long long)idx, a, (long long)s.dims[a]);
+        nvox *= s.dims[a];
+    }
+    CTLAB_REQUIRE(nvox < (1LL << 31), "batch: scan %lld has %lld voxels (limit 2^31)", (long long)idx,
+                  (long long)nvox);
+    CTLAB_REQUIRE(s.M_inv && s.b, "batch: scan %lld has a null M_inv or b", (long long)idx);
+    CTLAB_REQUIRE(s.n_ray == 0 || (s.src && s.dst), "batch: scan %lld has null src/dst", (long long)idx);
+    CTLAB_REQUIRE(s.image_in || s.sino_out || s.sino_in || s.image_out, "batch: scan %lld binds no buffer",
+                  (long long)idx);
+    // A pass binds its image and its sinogram together; the sinogram of a
+    // scan without rays may be NULL (an empty buffer).
+    const bool fwd = s.image_in || s.sino_out, adj = s.sino_in || s.image_out;
+    CTLAB_REQUIRE(!fwd || (s.image_in && (s.sino_out || s.n_ray == 0)),
+                  "batch: scan %lld: image_in and sino_out must be given together", (long long)idx);
+    CTLAB_REQUIRE(!adj || (s.image_out && (s.sino_in || s.n_ray == 0)),
+                  "batch: scan %lld: sino_in and image_out must be given together", (long long)idx);
+    const int rule = s.opts.voxel_rule;
+    CTLAB_REQUIRE(rule == voxel_rule, "batch: scan %lld has voxel_rule %d, the batch's first scan has %d",
+                  (long long)idx, rule, voxel_rule);
+    CTLAB_REQUIRE(s.opts.block_threads == 0 || s.opts.block_threads == block_threads,
+                  "batch: scan %lld asks for %d threads per tile, the batch runs %d", (long long)idx,
+                  s.opts.block_threads, block_threads);
+    ctlab_ray_opts o = s.opts;
+    o.block_threads = block_threads;
+    Tiling T;
+    int rc = resolve_tiling(&o, s.n_ray, T);
+    if (rc) return rc;
+    D.image_in = s.image_in;
+    D.sino_out = s.sino_out;
+    D.sino_in = s.sino_in;
+    D.image_out = s.image_out;
+    D.src = s.src;
+    D.dst = s.dst;
+    D.M_inv = s.M_inv;
+    D.b = s.b;
+    D.n_ray = s.n_ray;
+    D.nvox = nvox;
+    D.T = T;
+    int64_t st = 1;
+    for (int a = 2; a >= 0; --a) {
+        D.n[a] = a < ndim ? (int)s.dims[a] : 1;
+        D.stride[a] = a < ndim ? (int)st : 0;
+        if (a < ndim) st *= s.dims[a];
+    }
+    if (s.n_ray == 0) D.T.n_blocks = 0;
+    return CTLAB_OK;
+}
+
+template <int NDIM, bool ADJ, bool MID>
+static const void* batched_fn() {
+    return reinterpret_cast<const void*>(&batched_kernel<NDIM, ADJ, MID>);
+}
+
+static const void* pick_kernel(int ndim, bool adj, bool mid) {
+    if (ndim == 2) {
+        if (adj) return mid ? batched_fn<2, true, true>() : batched_fn<2, true, false>();
+        return mid ? batched_fn<2, false, true>() : batched_fn<2, false, false>();
+    }
+    if (adj) return mid ? batched_fn<3, true, true>() : batched_fn<3, true, false>();
+    return mid ? batched_fn<3, false, true>() : batched_fn<3, false, false>();
+}
+
+static int default_ctas(const void* fn, int block_threads, int* n_cta) {
+    int dev = 0, sms = 0, per_sm = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    CTLAB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CTLAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block_threads, 0));
+    *n_cta = (per_sm < 1 ? 1 : per_sm) * sms;
+    return CTLAB_OK;
+}
+
+static int launch_batched(const ctlab_batch* plan, bool adj, int accumulate, int32_t n_cta, void* stream) {
+    const char* what = adj ? "back_project_batched" : "forward_project_batched";
+    CTLAB_REQUIRE(plan != nullptr && plan->workspace != nullptr, "%s: null plan", what);
+    CTLAB_REQUIRE(plan->n_scan >= 1 && (plan->ndim == 2 || plan->ndim == 3), "%s: plan is not initialised", what);
+    CTLAB_REQUIRE(adj ? plan->has_adjoint : plan->has_forward, "%s: the plan's scans bind no %s buffers", what,
+                  adj ? "adjoint" : "forward");
+    CTLAB_REQUIRE(n_cta >= 0, "%s: n_cta must be >= 0 (0 = resident CTAs per SM x SMs)", what);
+    int dev = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    CTLAB_REQUIRE(dev == plan->device, "%s: the plan was made on device %d, the current device is %d", what,
+                  plan->device, dev);
+    cudaStream_t s = as_stream(stream);
+    char* ws = static_cast<char*>(plan->workspace);
+    const ScanDev* table = reinterpret_cast<const ScanDev*>(ws + sizeof(BatchHeader));
+    unsigned* counter = reinterpret_cast<unsigned*>(ws);
+    if (adj && !accumulate) {
+        batched_zero_kernel<<<dim3(64, (unsigned)plan->n_scan), 256, 0, s>>>(table);
+        int rc = launch_status(what);
+        if (rc) return rc;
+    }
+    if (plan->total_tiles == 0) return CTLAB_OK;
+    const bool mid = plan->voxel_rule == CTLAB_VOXEL_MIDPOINT;
+    const void* fn = pick_kernel(plan->ndim, adj, mid);
+    int ctas = n_cta;
+    if (ctas == 0) {
+        int rc = default_ctas(fn, plan->block_threads, &ctas);
+        if (rc) return rc;
+    }
+    CTLAB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+    const unsigned total = (unsigned)plan->total_tiles;
+    const int n_scan = plan->n_scan;
+    void* args[] = {(void*)&table, (void*)&n_scan, (void*)&total, (void*)&counter};
+    CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)plan->block_threads), args, 0, s));
+    return launch_status(what);
+}
+
+}  // namespace ctlab
+
+using namespace ctlab;
+
+extern "C" int64_t ctlab_batch_workspace_bytes(int32_t n_scan) {
+    if (n_scan < 1 || n_scan > kMaxBatchScans) return -1;
+    return (int64_t)sizeof(BatchHeader) + table_bytes(n_scan);
+}
+
+extern "C" int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t block_threads, void* workspace,
+                                int64_t workspace_bytes, ctlab_batch* plan, void* stream) {
+    clear_error();
+    CTLAB_REQUIRE(scans != nullptr && plan != nullptr, "batch_plan: null scans or plan");
+    CTLAB_REQUIRE(n_scan >= 1 && n_scan <= kMaxBatchScans, "batch_plan: n_scan must be in [1, %lld] (got %d)",
+                  (long long)kMaxBatchScans, n_scan);
+    if (block_threads == 0) block_threads = 256;
+    CTLAB_REQUIRE(block_threads >= 32 && block_threads <= 256 && block_threads % 32 == 0,
+                  "batch_plan: block_threads must be a multiple of 32 in [32, 256] (got %d)", block_threads);
+    const int64_t need = ctlab_batch_workspace_bytes(n_scan);
+    CTLAB_REQUIRE(workspace != nullptr && workspace_bytes >= need,
+                  "batch_plan: workspace of %lld bytes is too small (%lld needed for %d scans)",
+                  (long long)workspace_bytes, (long long)need, n_scan);
+    CTLAB_REQUIRE((reinterpret_cast<uintptr_t>(workspace) & 255u) == 0, "batch_plan: workspace must be 256-byte aligned");
+    const int ndim = scans[0].ndim;
+    CTLAB_REQUIRE(ndim == 2 || ndim == 3, "batch_plan: ndim must be 2 or 3 (got %d)", ndim);
+    const int rule = scans[0].opts.voxel_rule;
+    CTLAB_REQUIRE(rule == CTLAB_VOXEL_MIDPOINT || rule == CTLAB_VOXEL_CROSSING, "batch_plan: unknown voxel_rule %d",
+                  rule);
+    std::vector<ScanDev> table((size_t)n_scan);
+    int64_t tiles = 0;
+    bool fwd = false, adj = false;
+    for (int32_t i = 0; i < n_scan; ++i) {
+        int rc = resolve_scan(scans[i], i, ndim, block_threads, rule, table[i]);
+        if (rc) return rc;
+        table[i].first_tile = tiles;
+        tiles += table[i].T.n_blocks;
+        CTLAB_REQUIRE(tiles < kMaxBatchTiles, "batch_plan: more than 2^31 tiles in one batch");
+        fwd = fwd || scans[i].image_in != nullptr;
+        adj = adj || scans[i].image_out != nullptr;
+    }
+    int dev = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    char* ws = static_cast<char*>(workspace);
+    cudaStream_t s = as_stream(stream);
+    CTLAB_CUDA_TRY(cudaMemsetAsync(ws, 0, sizeof(BatchHeader), s));
+    // From pageable host memory: the call returns once the table has been
+    // staged, so `table` may be released right after it.
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(ws + sizeof(BatchHeader), table.data(), sizeof(ScanDev) * (size_t)n_scan,
+                                   cudaMemcpyHostToDevice, s));
+    plan->workspace = workspace;
+    plan->total_tiles = tiles;
+    plan->n_scan = n_scan;
+    plan->ndim = ndim;
+    plan->block_threads = block_threads;
+    plan->voxel_rule = rule;
+    plan->has_forward = fwd ? 1 : 0;
+    plan->has_adjoint = adj ? 1 : 0;
+    plan->device = dev;
+    plan->reserved = 0;
+    return CTLAB_OK;
+}
+
+extern "C" int ctlab_forward_project_batched(const ctlab_batch* plan, int32_t n_cta, void* stream) {
+    clear_error();
+    return launch_batched(plan, false, 0, n_cta, stream);
+}
+
+extern "C" int ctlab_back_project_batched(const ctlab_batch* plan, int accumulate, int32_t n_cta, void* stream) {
+    clear_error();
+    return launch_batched(plan, true, accumulate, n_cta, stream);
+}
+
+extern "C" int ctlab_batch_default_ctas(int32_t ndim, int adjoint, int voxel_rule, int32_t block_threads,
+                                        int32_t* n_cta) {
+    clear_error();
+    CTLAB_REQUIRE(n_cta != nullptr, "batch_default_ctas: null output");
+    CTLAB_REQUIRE(ndim == 2 || ndim == 3, "batch_default_ctas: ndim must be 2 or 3");
+    CTLAB_REQUIRE(block_threads >= 32 && block_threads <= 256 && block_threads % 32 == 0,
+                  "batch_default_ctas: block_threads must be a multiple of 32 in [32, 256]");
+    int v = 0;
+    int rc = default_ctas(pick_kernel(ndim, adjoint != 0, voxel_rule == CTLAB_VOXEL_MIDPOINT), block_threads, &v);
+    if (rc) return rc;
+    *n_cta = v;
+    return CTLAB_OK;
+}

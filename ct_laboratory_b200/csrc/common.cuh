@@ -173,10 +173,10 @@ int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& out);
 // moment share one band of detector rows across many views; for a cone-beam
 // scan such a band sees a slab of the volume about tile_rows detector rows
 // thick, and the volume voxels the whole GPU touches at a time stay a small,
-// L2-resident fraction of the volume.  The launch has at most 2^31 - 1
-// blocks, so all tile coordinates fit 32-bit unsigned division.
-__device__ __forceinline__ int64_t tile_ray(const Tiling& T) {
-    const unsigned blk = blockIdx.x;
+// L2-resident fraction of the volume.  A scan has at most 2^31 - 1 tiles,
+// so all tile coordinates fit 32-bit unsigned division.  `blk` is the tile
+// index (the block index of a one-scan launch).
+__device__ __forceinline__ int64_t tile_ray_at(const Tiling& T, unsigned blk) {
     const unsigned per_band = (unsigned)(T.n_view * T.tiles_c);
     const unsigned tr_u = blk / per_band;
     const unsigned rem = blk - tr_u * per_band;
@@ -189,5 +189,7 @@ __device__ __forceinline__ int64_t tile_ray(const Tiling& T) {
     if (row >= T.n_row || col >= T.n_col) return -1;
     return view * T.view_stride + row * T.row_stride + col * T.col_stride;
 }
+
+__device__ __forceinline__ int64_t tile_ray(const Tiling& T) { return tile_ray_at(T, blockIdx.x); }
 
 }  // namespace ctlab

@@ -1,0 +1,723 @@
+#pragma once
+// walk.cuh — device side of the Siddon walks (sm_100a), shared by the
+// single-scan kernels (siddon.cu) and the multi-scan persistent kernels
+// (batched.cu): the on-the-fly Siddon forward projector and its exact adjoint,
+// 2-D and 3-D.
+//
+// The reference's on-the-fly 3-D kernel (src/ct_projector_3d.cu:902-1012)
+// collects every plane hit of a ray into an 8 KB per-thread array, insertion-
+// sorts it and then walks the sorted list.  The x-, y- and z-plane parameters
+// of a ray are each already monotone, so their sorted union is a three-way
+// merge.  The walk here takes that merge directly (a DDA): it keeps the next
+// plane parameter of every axis in registers, repeatedly takes the smallest,
+// and evaluates each plane's parameter on its own with the reference's
+// formula t = (p - s) * (1/v), so the segment end points are the very floats
+// the reference sorts.  Only segments inside the volume are visited (those
+// outside map to out-of-range voxels, which the reference skips).  The voxel
+// of a segment comes from which planes were crossed rather than from rounding
+// the segment midpoint; the two agree except for segments of rounding-noise
+// length, which contribute rounding-noise amounts.
+//
+// Memory behaviour: the volume is read through the read-only path with an
+// L2 evict-last policy and the ray geometry and sinogram stream through with
+// evict-first, so that a volume the size of the benchmark's (256^3 fp32 =
+// 64 MiB) stays resident in the 126 MB L2.  A CTA covers `tile_rows` detector rows x (threads/tile_rows)
+// columns, with warp lanes along rows, so that for a cone-beam scan the 32
+// lanes of a warp trace 32 vertically adjacent rays: they share the same x-y
+// path and touch neighbouring k (fastest-varying) voxels, so a warp's gather
+// hits a few 32-byte sectors instead of 32.  The adjoint scatters with
+// red.global.add.f32 (atomicAdd with an unused result).
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace ctlab {
+
+template <int NDIM>
+using AffineT = typename std::conditional<NDIM == 3, Affine3, Affine2>::type;
+
+template <int NDIM>
+struct GridDims {
+    int n[NDIM];
+    int stride[NDIM];
+};
+
+// Round half to even to int without a conversion instruction: adding
+// 1.5*2^23 leaves the rounded integer in the low mantissa bits (exact for
+// |x| < 2^22); outside that range (and for NaN / inf) the result is an
+// integer >= 2^22 or negative, which every grid bound check (n <= 2^22)
+// rejects.
+__device__ __forceinline__ int rne_int(float x) {
+    return __float_as_int(__fadd_rn(x, 12582912.0f)) - 0x4B400000;
+}
+
+// Voxel of a segment [t0, t1] under the reference's rule: the world-space
+// midpoint s + t_mid*v mapped to index space and rounded half to even
+// (ct_projector_3d.cu:982-996).  Returns the flat index or -1 (outside).
+template <int NDIM>
+__device__ __forceinline__ int midpoint_voxel(const AffineT<NDIM>& A, const float* sw, const float* vw, float t0,
+                                              float t1, const GridDims<NDIM>& G) {
+    const float tm = __fmul_rn(0.5f, __fadd_rn(t0, t1));
+    float m[NDIM], f[NDIM];
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) m[a] = __fmaf_rn(tm, vw[a], sw[a]);
+    if constexpr (NDIM == 3) world_to_index3(A, m[0], m[1], m[2], f[0], f[1], f[2]);
+    else world_to_index2(A, m[0], m[1], f[0], f[1]);
+    int flat = 0;
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        const int i = rne_int(f[a]);
+        ok = ok && (unsigned)i < (unsigned)G.n[a];
+        flat += i * G.stride[a];
+    }
+    return ok ? flat : -1;
+}
+
+// Segments next to the grid under the midpoint rule.  The reference forms a
+// segment between every two consecutive plane hits in [0, 1] (the end points
+// 0 and 1 included, ct_projector_3d.cu:889-891) and charges it to the voxel
+// its rounded float midpoint falls in (:982-996).  Segments before the entry
+// or after the exit lie outside the grid, but one thinner than the rounding
+// noise of the midpoint (about 1e-4 voxel at scanner coordinates) can have
+// its midpoint rounded onto a face voxel.  This finds the segments the
+// reference forms next to the entry (DIR = -1, from t_edge = t_enter
+// backwards) or the exit (DIR = +1, from t_edge = t_exit onwards): the
+// neighbouring hits are the next in-range plane of each axis beyond the
+// edge, or the end point.  It records up to kEdge of them, nearest first,
+// and stops at the first whose midpoint rounds outside the grid.  p0[a] is a
+// plane of axis a at or beyond the edge (its parameter on the far side of
+// t_edge or equal to it).
+constexpr int kEdge = 2;
+
+template <int NDIM, int DIR>
+__device__ __forceinline__ int edge_segments(const AffineT<NDIM>& A, const float* sw, const float* vw,
+                                             const float* s, const float* inv, const float* ps, const float* p0,
+                                             float t_edge, float ray_len, const GridDims<NDIM>& G, int* vox,
+                                             float* len) {
+    const float kFar = DIR > 0 ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
+#pragma unroll
+    for (int k = 0; k < kEdge; ++k) {
+        vox[k] = 0;
+        len[k] = 0.f;
+    }
+    float q[NDIM], tq[NDIM];
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        q[a] = p0[a];
+        tq[a] = kFar;
+        if (inv[a] == 0.f) continue;
+        tq[a] = plane_t(q[a], s[a], inv[a]);
+        // a plane at the edge itself bounds no segment on this side: step past it
+#pragma unroll 1
+        for (int k = 0; k < 2 && (DIR > 0 ? tq[a] <= t_edge : tq[a] >= t_edge); ++k) {
+            q[a] += (float)DIR * ps[a];
+            tq[a] = plane_t(q[a], s[a], inv[a]);
+        }
+        const bool in = q[a] >= -0.5f && q[a] <= (float)G.n[a] - 0.5f;
+        if (!in || (DIR > 0 ? tq[a] <= t_edge : tq[a] >= t_edge)) tq[a] = kFar;
+    }
+    int n = 0;
+    float t_near = t_edge;
+#pragma unroll
+    for (int k = 0; k < kEdge; ++k) {
+        if (DIR > 0 ? !(t_near < 1.f) : !(t_near > 0.f)) break;
+        float t_far = DIR > 0 ? 1.f : 0.f;
+#pragma unroll
+        for (int a = 0; a < NDIM; ++a) t_far = DIR > 0 ? fminf(t_far, tq[a]) : fmaxf(t_far, tq[a]);
+        const float lo = DIR > 0 ? t_near : t_far, hi = DIR > 0 ? t_far : t_near;
+        const int m = midpoint_voxel<NDIM>(A, sw, vw, lo, hi, G);
+        if (m < 0) break;
+        vox[n] = m;
+        len[n] = __fmul_rn(__fsub_rn(hi, lo), ray_len);
+        ++n;
+#pragma unroll
+        for (int a = 0; a < NDIM; ++a) {
+            if (tq[a] == t_far) {
+                q[a] += (float)DIR * ps[a];
+                const bool in = q[a] >= -0.5f && q[a] <= (float)G.n[a] - 0.5f;
+                tq[a] = in ? plane_t(q[a], s[a], inv[a]) : kFar;
+            }
+        }
+        t_near = t_far;
+    }
+    return n;
+}
+
+// One Siddon traversal.  ADJ=false: returns sum of in[voxel]*len.
+// ADJ=true: scatters y*len into out[voxel].  MID selects the voxel of each
+// segment: true = the reference's rounded world midpoint, false = the voxel
+// between the two crossings that bound the segment (exact topology).
+template <int NDIM, bool ADJ, bool MID>
+__device__ __forceinline__ float traverse(const float* __restrict__ vol, float* __restrict__ out, float y,
+                                          const float* sw, const float* dw, const GridDims<NDIM>& G,
+                                          const AffineT<NDIM>& A, unsigned nvox) {
+    // World direction and length: ct_projector_3d.cu:941-942 (fused as nvcc
+    // contracts vx*vx + vy*vy + vz*vz).
+    float vw[NDIM];
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
+    float len2;
+    if constexpr (NDIM == 3) len2 = sumsq3(vw[0], vw[1], vw[2]);
+    else len2 = sumsq2(vw[0], vw[1]);
+    const float ray_len = sqrtf(len2);
+    if (!(ray_len >= 1e-12f)) return 0.f;
+
+    // Endpoints in index space.
+    float s[NDIM], d[NDIM];
+    if constexpr (NDIM == 3) {
+        world_to_index3(A, sw[0], sw[1], sw[2], s[0], s[1], s[2]);
+        world_to_index3(A, dw[0], dw[1], dw[2], d[0], d[1], d[2]);
+    } else {
+        world_to_index2(A, sw[0], sw[1], s[0], s[1]);
+        world_to_index2(A, dw[0], dw[1], d[0], d[1]);
+    }
+
+    float inv[NDIM], tn[NDIM], pn[NDIM], ps[NDIM];
+    int ds[NDIM];
+    float t_enter = 0.f, t_exit = 1.f;
+    int idx = 0;
+    bool live = true;
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        const float va = __fsub_rn(d[a], s[a]);
+        const float nf = (float)G.n[a];
+        live = live && isfinite(s[a]) && isfinite(va);
+        if (fabsf(va) > 1e-12f) {
+            // collect_hits (ct_projector_3d.cu:865-870): inv = 1/v.
+            inv[a] = __frcp_rn(va);
+            const float lo = va > 0.f ? -0.5f : nf - 0.5f;
+            const float hi = va > 0.f ? nf - 0.5f : -0.5f;
+            t_enter = fmaxf(t_enter, plane_t(lo, s[a], inv[a]));
+            t_exit = fminf(t_exit, plane_t(hi, s[a], inv[a]));
+            ps[a] = va > 0.f ? 1.f : -1.f;
+            ds[a] = va > 0.f ? G.stride[a] : -G.stride[a];
+        } else {
+            // No planes of this axis are hit: the ray keeps one index along
+            // it, the rounded coordinate (the reference rounds the midpoint).
+            inv[a] = 0.f;
+            const int i = __float2int_rn(s[a]);
+            live = live && (i >= 0) && (i < G.n[a]);
+            idx += i * G.stride[a];
+            tn[a] = __int_as_float(0x7f800000);  // +inf
+            pn[a] = 0.f;
+            ps[a] = 0.f;
+            ds[a] = 0;
+        }
+    }
+    live = live && (t_enter < t_exit);
+    if (!live) return 0.f;
+
+    // Starting voxel: for each crossing axis, the slab whose behind-plane
+    // parameter is <= t_enter and whose ahead-plane parameter is > t_enter,
+    // found from an estimate and fixed up with the exact plane formula.
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        if (inv[a] == 0.f) continue;
+        const float va = __fsub_rn(d[a], s[a]);
+        const float c = __fmaf_rn(t_enter, va, s[a]);
+        int i = __float2int_rd(c + 0.5f);
+        if (va > 0.f) {
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s[a], inv[a]) <= t_enter; ++k) ++i;
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s[a], inv[a]) > t_enter; ++k) --i;
+        } else {
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s[a], inv[a]) <= t_enter; ++k) --i;
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s[a], inv[a]) > t_enter; ++k) ++i;
+        }
+        i = min(max(i, 0), G.n[a] - 1);
+        idx += i * G.stride[a];
+        pn[a] = (float)i + 0.5f * ps[a];
+        tn[a] = plane_t(pn[a], s[a], inv[a]);
+    }
+
+    // The merge walk.  Each step ends the current segment at the nearest
+    // next plane (or at t_exit) and then steps every axis whose next plane
+    // lies exactly there: equal plane parameters of two axes only ever bound
+    // a zero-length segment, which the reference skips and which would add
+    // nothing here, so stepping them together gives the same segments.  The
+    // steps are predicated, not branched, so the lanes of a warp never
+    // diverge inside the walk.
+    //
+    // The voxel index never leaves the grid: an axis is stepped across its
+    // last plane only when that plane's parameter (>= t_exit, which is the
+    // minimum over the axes' exit planes) is below t_exit, which cannot
+    // happen.  Every plane is crossed at most once, which bounds the loop
+    // even for non-finite input.
+    int max_it = 3;
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) max_it += G.n[a];
+    (void)nvox;
+    float t_cur = t_enter;
+    if constexpr (!ADJ) {
+        // Forward: four steps, then their four gathers back to back (four
+        // loads in flight per lane), accumulated in walk order; zero-length
+        // segments (ties, and the padding after the exit) are not added.
+        float acc = 0.f;
+        bool done = false;
+        const uint64_t pol = l2_policy_keep();
+        if constexpr (MID) {
+            // segments just before the entry, added in ascending order
+            float pb[NDIM], el[kEdge];
+            int ev[kEdge];
+#pragma unroll
+            for (int a = 0; a < NDIM; ++a) pb[a] = pn[a] - ps[a];
+            const int ne = edge_segments<NDIM, -1>(A, sw, vw, s, inv, ps, pb, t_enter, ray_len, G, ev, el);
+#pragma unroll
+            for (int k = kEdge - 1; k >= 0; --k)
+                if (k < ne && el[k] > 0.f) acc = __fmaf_rn(ld_keep(vol + (unsigned)ev[k], pol), el[k], acc);
+        }
+#pragma unroll 1
+        for (int it = 0; it < max_it && !done; it += 4) {
+            int vq[4];
+            float sq[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float tm = tn[0];
+#pragma unroll
+                for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
+                const float t1 = fminf(tm, t_exit);
+                float seg = done ? 0.f : __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                int v = idx;
+                if constexpr (MID) {
+                    const int m = midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G);
+                    v = m < 0 ? 0 : m;
+                    seg = m < 0 ? 0.f : seg;
+                }
+                vq[q] = v;
+                sq[q] = seg;
+                done = done || !(tm < t_exit);
+                t_cur = t1;
+#pragma unroll
+                for (int a = 0; a < NDIM; ++a) {
+                    if (!done && tn[a] == tm) {
+                        idx += ds[a];
+                        pn[a] += ps[a];
+                        tn[a] = plane_t(pn[a], s[a], inv[a]);
+                    }
+                }
+            }
+            float vv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) vv[q] = ld_keep(vol + (unsigned)vq[q], pol);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc = sq[q] > 0.f ? __fmaf_rn(vv[q], sq[q], acc) : acc;
+        }
+        if constexpr (MID) {
+            // segments just after the exit
+            float el[kEdge];
+            int ev[kEdge];
+            const int ne = edge_segments<NDIM, 1>(A, sw, vw, s, inv, ps, pn, t_exit, ray_len, G, ev, el);
+#pragma unroll
+            for (int k = 0; k < kEdge; ++k)
+                if (k < ne && el[k] > 0.f) acc = __fmaf_rn(ld_keep(vol + (unsigned)ev[k], pol), el[k], acc);
+        }
+        return acc;
+    } else {
+        if constexpr (MID) {
+            float pb[NDIM], el[kEdge];
+            int ev[kEdge];
+#pragma unroll
+            for (int a = 0; a < NDIM; ++a) pb[a] = pn[a] - ps[a];
+            const int ne = edge_segments<NDIM, -1>(A, sw, vw, s, inv, ps, pb, t_enter, ray_len, G, ev, el);
+#pragma unroll
+            for (int k = 0; k < kEdge; ++k)
+                red_add_if(out + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
+        }
+#pragma unroll 1
+        for (int it = 0; it < max_it; ++it) {
+            float tm = tn[0];
+#pragma unroll
+            for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
+            const float t1 = fminf(tm, t_exit);
+            // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
+            const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+            const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
+            red_add_if(out + (unsigned)v, __fmul_rn(y, seg), seg > 0.f && v >= 0);
+            if (!(tm < t_exit)) break;
+            t_cur = t1;
+#pragma unroll
+            for (int a = 0; a < NDIM; ++a) {
+                if (tn[a] == tm) {
+                    idx += ds[a];
+                    pn[a] += ps[a];
+                    tn[a] = plane_t(pn[a], s[a], inv[a]);
+                }
+            }
+        }
+        if constexpr (MID) {
+            float el[kEdge];
+            int ev[kEdge];
+            const int ne = edge_segments<NDIM, 1>(A, sw, vw, s, inv, ps, pn, t_exit, ray_len, G, ev, el);
+#pragma unroll
+            for (int k = 0; k < kEdge; ++k)
+                red_add_if(out + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
+        }
+        return 0.f;
+    }
+}
+
+// Per-thread body of the per-lane walk: ray r (>= 0) of batch item bi.
+template <int NDIM, bool ADJ, bool MID>
+__device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __restrict__ out,
+                                         const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
+                                         const AffineT<NDIM>& aff, const GridDims<NDIM>& G, int64_t nvox, int64_t r,
+                                         int64_t bi) {
+    float sw[NDIM], dw[NDIM];
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+        sw[a] = ld_stream(src + r * NDIM + a);
+        dw[a] = ld_stream(dst + r * NDIM + a);
+    }
+    if constexpr (ADJ) {
+        const float y = ld_stream(in + bi * n_ray + r);
+        if (y == 0.f) return;  // contributes exactly nothing
+        traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
+    } else {
+        st_stream(out + bi * n_ray + r,
+                  traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox));
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Shared x-y walk for detector columns (3-D, crossing rule).
+//
+// When the 32 lanes of a warp trace rays that share their x-y line (one
+// source, one detector column whose cells run along z: cone-beam views and
+// StaticCT rings tiled with 32 detector rows per warp), every x- and y-plane
+// parameter is bitwise the same for all lanes and only the z planes differ.
+// The per-lane walk then spends most of its compare / select work deriving
+// the same x-y crossings 32 times over.  Here the warp derives the merged x-y
+// crossing sequence once, 32 crossings per round: lane l evaluates the l-th
+// next x plane and the l-th next y plane, a rank search across the warp
+// places each in merged order, and the first 32 go to a per-warp shared
+// buffer together with the x-y column each one ends.  Every lane then walks
+// the buffer cell by cell (the same cell on all lanes, a broadcast read) and
+// splits the cell at its own next z plane when one falls inside it:
+//     te = min(t_cell_end, t_exit)      ts = min(t_next_z, te)
+//     segment A = [t_cur, ts] in (column, k)
+//     segment B = [ts, te]    in (column, k +- 1), empty unless a z plane lies inside
+// Segments are (t1 - t0) * |v| over the same plane parameters as the per-lane
+// walk, taken in the same order, and zero-length ones are skipped as there,
+// so the results are bitwise those of traverse<3, ADJ, false>.
+//
+// At most one z plane per cell: a cell spans at most the x or y plane
+// spacing in t, 1 / max(|v_x|, |v_y|), and z planes are 1 / |v_z| apart.  A
+// warp takes this walk only when every live lane has |v_z| <= 0.75 max(|v_x|,
+// |v_y|) and |s| <= 2^17 (with every grid dimension <= 2^16, checked on the
+// host), so |p - s| < 2^18 and float rounding of a plane parameter (< 2^-6 of
+// a spacing) cannot close the 25 % margin.  Other warps run the per-lane walk.
+// ----------------------------------------------------------------------------
+constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
+constexpr int kGroup = 4;   // cells walked per inner step (kChunk is a multiple)
+
+struct XYCell {
+    float t;  // parameter of the crossing that ends the cell
+    int col;  // flat index of the cell's (i, j) column at k = 0
+};
+
+// Per-lane set-up, the arithmetic of the start of traverse<3>.
+struct LaneRay {
+    float s[3], va[3], inv[3], ray_len, t_enter, t_exit;
+    bool live;
+};
+
+__device__ __forceinline__ void lane_setup(LaneRay& R, const float* sw, const float* dw, const GridDims<3>& G,
+                                           const Affine3& A) {
+    float vw[3], d[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
+    R.ray_len = sqrtf(sumsq3(vw[0], vw[1], vw[2]));
+    R.live = R.ray_len >= 1e-12f;
+    world_to_index3(A, sw[0], sw[1], sw[2], R.s[0], R.s[1], R.s[2]);
+    world_to_index3(A, dw[0], dw[1], dw[2], d[0], d[1], d[2]);
+    R.t_enter = 0.f;
+    R.t_exit = 1.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float va = __fsub_rn(d[a], R.s[a]);
+        const float nf = (float)G.n[a];
+        R.va[a] = va;
+        R.live = R.live && isfinite(R.s[a]) && isfinite(va);
+        if (fabsf(va) > 1e-12f) {
+            R.inv[a] = __frcp_rn(va);
+            const float lo = va > 0.f ? -0.5f : nf - 0.5f;
+            const float hi = va > 0.f ? nf - 0.5f : -0.5f;
+            R.t_enter = fmaxf(R.t_enter, plane_t(lo, R.s[a], R.inv[a]));
+            R.t_exit = fminf(R.t_exit, plane_t(hi, R.s[a], R.inv[a]));
+        } else {
+            R.inv[a] = 0.f;
+            const int i = __float2int_rn(R.s[a]);
+            R.live = R.live && (i >= 0) && (i < G.n[a]);
+        }
+    }
+    R.live = R.live && (R.t_enter < R.t_exit);
+}
+
+// Slab of a crossing axis at parameter t: behind-plane parameter <= t and
+// ahead-plane parameter > t, from an estimate fixed up with the exact plane
+// formula (the start rule of traverse), clamped into the grid.
+__device__ __forceinline__ int slab_at(float t, float s, float va, float inv, int n) {
+    int i = __float2int_rd(__fmaf_rn(t, va, s) + 0.5f);
+    if (va > 0.f) {
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s, inv) <= t; ++k) ++i;
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s, inv) > t; ++k) --i;
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s, inv) <= t; ++k) --i;
+#pragma unroll 1
+        for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s, inv) > t; ++k) ++i;
+    }
+    return min(max(i, 0), n - 1);
+}
+
+// Number of lanes m whose `sorted` value (non-decreasing over the lanes) is
+// below `key` (INCLUSIVE: at or below): a branch-free binary search.
+template <bool INCLUSIVE>
+__device__ __forceinline__ int warp_rank(float sorted, float key) {
+    int c = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const float v = __shfl_sync(kFullMask, sorted, c + step - 1);
+        c += (INCLUSIVE ? v <= key : v < key) ? step : 0;
+    }
+    // c counts lanes 0..30; lane 31 is the one left to test
+    const float v = __shfl_sync(kFullMask, sorted, c);
+    return c + ((INCLUSIVE ? v <= key : v < key) ? 1 : 0);
+}
+
+// Per-lane z state of the shared x-y walk.
+struct ZWalk {
+    float t_cur, t_end, len, tnz, pnz, psz, s2, i2;
+    int kz, dsz;
+};
+
+// kGroup cells of the buffer from position q: segment A = [t_cur, ts] in
+// (column, k), segment B = [ts, te] in (column, k') after a z step.
+struct CellGroup {
+    float sa[kGroup], sb[kGroup];
+    unsigned ia[kGroup], ib[kGroup];  // voxel indices, valid where the segment is positive
+};
+
+__device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup& g, ZWalk& Z) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        const XYCell c = buf[q + u];
+        const float te = fminf(c.t, Z.t_end);
+        const float ts = fminf(Z.tnz, te);
+        g.sa[u] = __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len);
+        g.ia[u] = (unsigned)(c.col + Z.kz);
+        if (Z.tnz <= te) {  // a z plane inside the cell (or ending it)
+            Z.kz += Z.dsz;
+            Z.pnz += Z.psz;
+            Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
+        }
+        g.sb[u] = __fmul_rn(__fsub_rn(te, ts), Z.len);
+        g.ib[u] = (unsigned)(c.col + Z.kz);
+        Z.t_cur = fmaxf(Z.t_cur, te);
+    }
+}
+
+// A positive segment lies inside the lane's [t_enter, t_exit] and between
+// crossed planes only, so its voxel is inside the grid; zero-length ones
+// (before entry, after exit, ties) are neither read nor added.
+__device__ __forceinline__ void gather_group(const float* vol, const CellGroup& g, float* v, uint64_t pol) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        if (g.sa[u] > 0.f) v[u] = ld_keep(vol + g.ia[u], pol);
+        if (g.sb[u] > 0.f) v[kGroup + u] = ld_keep(vol + g.ib[u], pol);
+    }
+}
+
+__device__ __forceinline__ float accumulate_group(const CellGroup& g, const float* v, float acc) {
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+        if (g.sa[u] > 0.f) acc = __fmaf_rn(v[u], g.sa[u], acc);
+        if (g.sb[u] > 0.f) acc = __fmaf_rn(v[kGroup + u], g.sb[u], acc);
+    }
+    return acc;
+}
+
+// Per-thread body of the shared x-y walk: ray r of batch item bi (r = -1: the
+// thread has no ray but still takes part in the warp's collective steps).
+// All 32 lanes of the warp call it together; `buf` is the warp's kChunk-entry
+// shared-memory cell buffer.
+template <bool ADJ>
+__device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, float* __restrict__ out,
+                                              const float* __restrict__ src, const float* __restrict__ dst,
+                                              int64_t n_ray, const Affine3& A, const GridDims<3>& G,
+                                              int64_t nvox, int64_t r, int64_t bi, XYCell* buf) {
+    const int lane = threadIdx.x & 31;
+    float sw[3] = {0.f, 0.f, 0.f}, dw[3] = {0.f, 0.f, 0.f};
+    if (r >= 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            sw[a] = ld_stream(src + r * 3 + a);
+            dw[a] = ld_stream(dst + r * 3 + a);
+        }
+    }
+    float y = 0.f;
+    if constexpr (ADJ) {
+        if (r >= 0) y = ld_stream(in + bi * n_ray + r);
+    }
+    LaneRay R;
+    lane_setup(R, sw, dw, G, A);
+    R.live = R.live && (r >= 0) && (!ADJ || y != 0.f);
+
+    const unsigned live_mask = __ballot_sync(kFullMask, R.live);
+    if (live_mask == 0u) {
+        if (!ADJ && r >= 0) st_stream(out + bi * n_ray + r, 0.f);
+        return;
+    }
+    // Do the live lanes share their x-y line, and is every live lane's z
+    // slope inside the one-z-plane-per-cell bound?  (Dead lanes do not vote.)
+    const int leader = __ffs(live_mask) - 1;
+    const float s0 = __shfl_sync(kFullMask, R.s[0], leader), s1 = __shfl_sync(kFullMask, R.s[1], leader);
+    const float va0 = __shfl_sync(kFullMask, R.va[0], leader), va1 = __shfl_sync(kFullMask, R.va[1], leader);
+    const float i0 = __shfl_sync(kFullMask, R.inv[0], leader), i1 = __shfl_sync(kFullMask, R.inv[1], leader);
+    const float vxy = fmaxf(i0 != 0.f ? fabsf(va0) : 0.f, i1 != 0.f ? fabsf(va1) : 0.f);
+    const bool ok = !R.live || (__float_as_uint(R.s[0]) == __float_as_uint(s0) &&
+                                __float_as_uint(R.s[1]) == __float_as_uint(s1) &&
+                                __float_as_uint(R.va[0]) == __float_as_uint(va0) &&
+                                __float_as_uint(R.va[1]) == __float_as_uint(va1) &&
+                                fabsf(R.va[2]) <= 0.75f * vxy && fabsf(R.s[0]) <= 131072.f &&
+                                fabsf(R.s[1]) <= 131072.f && fabsf(R.s[2]) <= 131072.f);
+    if (!__all_sync(kFullMask, ok) || vxy == 0.f) {
+        if (r < 0) return;
+        if constexpr (ADJ) {
+            if (R.live) traverse<3, true, false>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
+        } else {
+            st_stream(out + bi * n_ray + r,
+                      R.live ? traverse<3, false, false>(in + bi * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
+                             : 0.f);
+        }
+        return;
+    }
+
+    // ---- x-y start, warp-uniform: the slabs at the earliest lane entry ----
+    const float kInf = __int_as_float(0x7f800000);
+    float t_start = R.live ? R.t_enter : kInf, t_stop = R.live ? R.t_exit : -kInf;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t_start = fminf(t_start, __shfl_xor_sync(kFullMask, t_start, o));
+        t_stop = fmaxf(t_stop, __shfl_xor_sync(kFullMask, t_stop, o));
+    }
+    int col = 0, dsx = 0, dsy = 0;
+    float pnx = 0.f, pny = 0.f, psx = 0.f, psy = 0.f;
+    if (i0 != 0.f) {
+        const int i = slab_at(t_start, s0, va0, i0, G.n[0]);
+        psx = va0 > 0.f ? 1.f : -1.f;
+        dsx = va0 > 0.f ? G.stride[0] : -G.stride[0];
+        pnx = (float)i + 0.5f * psx;
+        col += i * G.stride[0];
+    } else {
+        col += __float2int_rn(s0) * G.stride[0];
+    }
+    if (i1 != 0.f) {
+        const int j = slab_at(t_start, s1, va1, i1, G.n[1]);
+        psy = va1 > 0.f ? 1.f : -1.f;
+        dsy = va1 > 0.f ? G.stride[1] : -G.stride[1];
+        pny = (float)j + 0.5f * psy;
+        col += j * G.stride[1];
+    } else {
+        col += __float2int_rn(s1) * G.stride[1];
+    }
+
+    // ---- per-lane z state at the lane's own entry ------------------------
+    // Dead lanes keep t_cur = t_end = 0 and no z plane: every segment they
+    // form has zero length.
+    ZWalk Z;
+    Z.s2 = R.s[2];
+    Z.i2 = R.inv[2];
+    Z.t_cur = 0.f;
+    Z.t_end = 0.f;
+    Z.len = 0.f;
+    Z.tnz = kInf;
+    Z.pnz = 0.f;
+    Z.psz = 0.f;
+    Z.kz = 0;
+    Z.dsz = 0;
+    if (R.live) {
+        Z.t_cur = R.t_enter;
+        Z.t_end = R.t_exit;
+        Z.len = R.ray_len;
+        if (Z.i2 != 0.f) {
+            const int k = slab_at(Z.t_cur, Z.s2, R.va[2], Z.i2, G.n[2]);
+            Z.psz = R.va[2] > 0.f ? 1.f : -1.f;
+            Z.dsz = R.va[2] > 0.f ? G.stride[2] : -G.stride[2];
+            Z.pnz = (float)k + 0.5f * Z.psz;
+            Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
+            Z.kz = k * G.stride[2];
+        } else {
+            Z.kz = __float2int_rn(Z.s2) * G.stride[2];
+        }
+    }
+
+    // ---- rounds of 32 x-y crossings ---------------------------------------
+    // Each round consumes 32 crossings of the x-y sequence; after
+    // n_x + n_y + 2 of them both exit planes lie behind, so the bound below
+    // is never the reason the loop ends.
+    const float* __restrict__ vol = ADJ ? nullptr : pin_ptr(in + bi * nvox);
+    float* __restrict__ vout = ADJ ? pin_ptr(out + bi * nvox) : nullptr;
+    float acc = 0.f;
+    const uint64_t pol = l2_policy_keep();
+    const float fl = (float)lane;
+    const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
+#pragma unroll 1
+    for (int round = 0; round < max_rounds; ++round) {
+        // lane l: the l-th next x plane and the l-th next y plane (plane
+        // coordinates are exact: |p| < 2^17 in steps of 1)
+        const float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
+        const float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
+        // merged positions; on equal parameters the x crossing comes first
+        const int rx = lane + warp_rank<false>(ty, tx);
+        const int ry = lane + warp_rank<true>(tx, ty);
+        if (rx < kChunk) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
+        if (ry < kChunk) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
+        const int n_x = __popc(__ballot_sync(kFullMask, rx < kChunk));
+        __syncwarp();
+        // cells up to and including the one that ends at or after t_stop
+        const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
+        const int n_cells = min(n_in + 1, kChunk);
+        if constexpr (ADJ) {
+#pragma unroll 1
+            for (int q = 0; q < n_cells; q += kGroup) {
+                CellGroup g;
+                walk_group(buf, q, g, Z);
+#pragma unroll
+                for (int u = 0; u < kGroup; ++u) {
+                    red_add_if(vout + g.ia[u], __fmul_rn(y, g.sa[u]), g.sa[u] > 0.f);
+                    red_add_if(vout + g.ib[u], __fmul_rn(y, g.sb[u]), g.sb[u] > 0.f);
+                }
+            }
+        } else {
+            // the group's gathers are issued together (up to 2 * kGroup in
+            // flight), then accumulated in walk order
+#pragma unroll 1
+            for (int q = 0; q < n_cells; q += kGroup) {
+                CellGroup g;
+                float v[2 * kGroup];
+                walk_group(buf, q, g, Z);
+                gather_group(vol, g, v, pol);
+                acc = accumulate_group(g, v, acc);
+            }
+        }
+        if (n_in < kChunk) break;
+        __syncwarp();  // every lane is done with this round's cells
+        col += n_x * dsx + (kChunk - n_x) * dsy;
+        pnx = __fmaf_rn((float)n_x, psx, pnx);
+        pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
+    }
+    if constexpr (!ADJ) {
+        if (r >= 0) st_stream(out + bi * n_ray + r, acc);
+    }
+}
+
+
+}  // namespace ctlab

@@ -266,6 +266,87 @@ int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray
                                  int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
                                  void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* Many scans in one launch                                                */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * One scan of a batch: its geometry, its voxel grid and the buffers a
+ * forward and / or an adjoint pass read and write (batch size 1 per scan;
+ * layouts as above).  The forward reads image_in and writes sino_out; the
+ * adjoint reads sino_in and writes (or adds into) image_out.  Either pair may
+ * be NULL when that pass is not run; a scan with n_ray = 0 may give NULL
+ * sinogram pointers.  `opts` is the scan's ray tiling and
+ * voxel rule as for the single-scan *_ex calls (n_view = 0: flat); every scan
+ * of a batch has the same ndim and voxel rule, and opts.block_threads is 0 or
+ * the batch's.  opts.walk is not used: 3-D crossing-rule scans take the
+ * column walk in every warp whose rays share their x-y line and the per-lane
+ * walk elsewhere, which give bitwise equal results.
+ */
+typedef struct ctlab_scan {
+    const float* image_in;
+    float* sino_out;
+    const float* sino_in;
+    float* image_out;
+    const float* src;
+    const float* dst;
+    const float* M_inv;
+    const float* b;
+    int64_t n_ray;
+    int64_t dims[3]; /* 2-D: n_row, n_col (dims[2] unused); 3-D: n_x, n_y, n_z (each <= 65536) */
+    int32_t ndim;    /* 2 or 3 */
+    int32_t reserved;
+    ctlab_ray_opts opts;
+} ctlab_scan;
+
+/* A plan: filled by ctlab_batch_plan, owned by the caller, read by the
+ * launch calls.  `workspace` is the caller's device buffer that holds the
+ * work counter and the resolved scan table. */
+typedef struct ctlab_batch {
+    void* workspace;
+    int64_t total_tiles;
+    int32_t n_scan, ndim, block_threads, voxel_rule;
+    int32_t has_forward, has_adjoint;
+    int32_t device, reserved;
+} ctlab_batch;
+
+/* Bytes of device workspace a plan of n_scan scans needs (-1 if n_scan is
+ * outside [1, 65535]). */
+int64_t ctlab_batch_workspace_bytes(int32_t n_scan);
+
+/* Validates the scans (host array) and copies their resolved table into
+ * `workspace` (device memory, 256-byte aligned, at least
+ * ctlab_batch_workspace_bytes(n_scan) bytes) on `stream`; fills *plan.  Every
+ * scan is cut into tiles of block_threads rays (0 = 256); tiles are handed
+ * out in scan order, so list the heaviest scans first.  The plan stays valid
+ * while the workspace and every bound buffer stay allocated.  The table is
+ * copied from pageable memory (the call waits for the stream), so call this
+ * outside stream capture.
+ *
+ * No counterpart in the reference, whose projectors take one scan per call
+ * (src/bindings.cpp:65-104); it batches the calls that
+ * ctlab_forward_project_3d_on_the_fly_ex / ctlab_forward_project_2d_siddon
+ * (and their adjoints) make one at a time, with their results: bitwise for
+ * the forward, up to the order of the float atomic additions for the adjoint. */
+int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t block_threads, void* workspace,
+                     int64_t workspace_bytes, ctlab_batch* plan, void* stream);
+
+/* One persistent launch of n_cta CTAs (0 = resident CTAs per SM x SMs) that
+ * projects every scan of the plan: sino_out = A image_in.  Resets the
+ * plan's work counter on the stream first (cudaMemsetAsync), so launches of
+ * one plan on one stream may follow each other, and may be captured in a
+ * CUDA graph; launches of one plan on two streams at once race. */
+int ctlab_forward_project_batched(const ctlab_batch* plan, int32_t n_cta, void* stream);
+
+/* image_out = A^T sino_in for every scan of the plan (accumulate = 0 zeroes
+ * each image_out first, 1 adds into it); one zeroing launch (if any) and one
+ * persistent launch. */
+int ctlab_back_project_batched(const ctlab_batch* plan, int accumulate, int32_t n_cta, void* stream);
+
+/* Resident CTAs per SM x SMs of the current device for the batched kernel
+ * of this kind (ndim, adjoint 0/1, voxel rule, block_threads). */
+int ctlab_batch_default_ctas(int32_t ndim, int adjoint, int voxel_rule, int32_t block_threads, int32_t* n_cta);
+
 #ifdef __cplusplus
 }
 #endif

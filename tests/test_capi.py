@@ -60,6 +60,38 @@ def test_validation_without_gpu():
     assert rc == 1 and b"tiling" in lib.ctlab_last_error()
 
 
+def test_batch_plan_validation_without_gpu():
+    from ct_laboratory_b200 import _native as N
+    lib = N.lib
+    assert lib.ctlab_batch_workspace_bytes(0) == -1 and lib.ctlab_batch_workspace_bytes(65536) == -1
+    assert lib.ctlab_batch_workspace_bytes(4) >= 256 + 4 * 64
+    fake = 256 * 1024  # never dereferenced: validation fails first
+    scans = (N.Scan * 2)()
+    for s in scans:
+        s.ndim, s.n_ray, s.src, s.dst, s.M_inv, s.b = 2, 10, fake, fake, fake, fake
+        s.image_in, s.sino_out = fake, fake
+        s.dims[0], s.dims[1] = 8, 8
+    plan = N.Batch()
+    need = lib.ctlab_batch_workspace_bytes(2)
+    rc = lib.ctlab_batch_plan(scans, 2, 256, ctypes.c_void_p(fake), need - 1, ctypes.byref(plan), None)
+    assert rc == 1 and b"too small" in lib.ctlab_last_error()
+    rc = lib.ctlab_batch_plan(scans, 2, 100, ctypes.c_void_p(fake), need, ctypes.byref(plan), None)
+    assert rc == 1 and b"block_threads" in lib.ctlab_last_error()
+    scans[1].ndim = 3
+    rc = lib.ctlab_batch_plan(scans, 2, 256, ctypes.c_void_p(fake), need, ctypes.byref(plan), None)
+    assert rc == 1 and b"ndim" in lib.ctlab_last_error()
+    scans[1].ndim = 2
+    scans[1].opts.voxel_rule = 1
+    rc = lib.ctlab_batch_plan(scans, 2, 256, ctypes.c_void_p(fake), need, ctypes.byref(plan), None)
+    assert rc == 1 and b"voxel_rule" in lib.ctlab_last_error()
+    scans[1].opts.voxel_rule = 0
+    scans[1].sino_out = None
+    rc = lib.ctlab_batch_plan(scans, 2, 256, ctypes.c_void_p(fake), need, ctypes.byref(plan), None)
+    assert rc == 1 and b"together" in lib.ctlab_last_error()
+    rc = lib.ctlab_forward_project_batched(ctypes.byref(N.Batch()), 0, None)
+    assert rc == 1 and b"plan" in lib.ctlab_last_error()
+
+
 def test_product_does_not_import_oracle():
     pkg = os.path.join(ROOT, "ct_laboratory_b200")
     for dirpath, _, files in os.walk(pkg):

@@ -1,0 +1,112 @@
+"""Speed and full-size parity against the reference's own CUDA projector.
+
+The reference's default cone-beam path is its on-the-fly kernel
+(ConeBeam3DProjector defaults to precomputed_intersections=False,
+conebeam_projector_3d.py:129; kernel ray_kernel_plane_sort,
+src/ct_projector_3d.cu:902-1012), compiled from its sources into oracle/_ref
+by oracle/build_ref.py.  Here it runs on an evenly spaced sample of the
+views of the cone-beam 256^3 benchmark scan (0.5 mm voxels, 360 views,
+512 x 384 cells at 0.8 mm, SID 1000 mm / SDD 1500 mm): its cost per ray is
+independent of the other rays, so rays per second on the sample stand for
+the whole scan.  Ours runs the whole scan the way the benchmark does
+(crossing voxel rule, column walk, L2 flushed before each pass).
+
+The reference's adjoint is called through _C with the correct M^-1 (its
+Python wrapper would invert twice, ct_projector_3d_cuda.py:209-210, :319).
+
+Set CTLAB_PERF_OUT=<file> to have the measured figures written as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+SAMPLE_VIEWS = (0, 90, 180, 270)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle.build_ref import load_ref
+    mod = load_ref()
+    if mod is None:
+        pytest.skip("reference CUDA build not present (python oracle/build_ref.py)")
+    return mod
+
+
+def _events_ms(fn, reps, flush=None):
+    out = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.median(out))
+
+
+def test_cone256_speed_and_parity_vs_reference_cuda(ref):
+    from ct_laboratory_b200 import ConeBeam3DProjector, _C
+    from ct_laboratory_b200.workloads import WORKLOADS
+    w = WORKLOADS["cone256"]
+    x = w.phantom(device=DEV)
+    proj = ConeBeam3DProjector(*w.n, n_view=w.n_view, det_nx=w.det_nx, det_ny=w.det_ny, sid=w.sid, sdd=w.sdd,
+                               det_spacing=w.pitch, voxel_size=w.voxel, device=DEV, voxel_rule=1)
+    n_ray = proj.src.shape[0]
+    y = torch.rand(n_ray, device=DEV, generator=torch.Generator(device=DEV).manual_seed(1))
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=DEV)
+    with torch.no_grad():
+        for _ in range(3):
+            proj.forward_project(x)
+            proj.back_project(y)
+        torch.cuda.synchronize()
+        t_fwd = _events_ms(lambda: proj.forward_project(x), 5, flush)
+        t_adj = _events_ms(lambda: proj.back_project(y), 5, flush)
+    ours_rate = n_ray / ((t_fwd + t_adj) / 1e3)
+
+    # the sample: whole views, contiguous in the [view][v][u] ray order
+    per_view = w.det_nx * w.det_ny
+    idx = torch.cat([torch.arange(v * per_view, (v + 1) * per_view, device=DEV) for v in SAMPLE_VIEWS])
+    src, dst = proj.src[idx].contiguous(), proj.dst[idx].contiguous()
+    ys = y[idx].contiguous()
+    Mi = torch.inverse(proj.M).contiguous()
+    b = proj.b
+    n_s = idx.numel()
+    # warm-up on one view, then one timed pass over the sample
+    ref.forward_project_3d_on_the_fly_cuda(x, src[:per_view], dst[:per_view], Mi, b)
+    ref.back_project_3d_on_the_fly_cuda(ys[:per_view], src[:per_view], dst[:per_view], Mi, b, *w.n)
+    torch.cuda.synchronize()
+    holder = {}
+    r_fwd = _events_ms(lambda: holder.__setitem__("f", ref.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b)), 1)
+    r_adj = _events_ms(lambda: holder.__setitem__("b", ref.back_project_3d_on_the_fly_cuda(ys, src, dst, Mi, b,
+                                                                                            *w.n)), 1)
+    ref_rate = n_s / ((r_fwd + r_adj) / 1e3)
+    ratio = ours_rate / ref_rate
+
+    # parity at full size on the sampled views: our kernels with the
+    # reference's voxel rule (midpoint) against the reference's kernels
+    ours_f = _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b)
+    e_f = rel_err(ours_f.cpu().numpy(), holder["f"].cpu().numpy())
+    ours_b = _C.back_project_3d_on_the_fly_cuda(ys, src, dst, Mi, b, *w.n)
+    e_b = rel_err(ours_b.cpu().numpy(), holder["b"].cpu().numpy())
+
+    res = {"workload": "cone256", "n_ray": n_ray, "ours_ms_fwd": t_fwd, "ours_ms_adj": t_adj,
+           "ours_grays_s": ours_rate / 1e9, "ref_sample_views": list(SAMPLE_VIEWS), "ref_sample_rays": n_s,
+           "ref_ms_fwd_sample": r_fwd, "ref_ms_adj_sample": r_adj, "ref_grays_s": ref_rate / 1e9,
+           "ref_ms_fwd_full_extrapolated": r_fwd * n_ray / n_s, "ref_ms_adj_full_extrapolated": r_adj * n_ray / n_s,
+           "speedup": ratio, "parity_fwd_rel": e_f, "parity_adj_rel": e_b}
+    print(json.dumps(res))
+    out = os.environ.get("CTLAB_PERF_OUT")
+    if out:
+        with open(out, "w") as f:
+            json.dump(res, f, indent=1)
+    assert e_f < 1e-5 and e_b < 1e-5, res
+    assert ratio >= 10.0, res
