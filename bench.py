@@ -48,6 +48,7 @@ sys.path.insert(0, ROOT)
 SEGMENTS = {
     "fan256": 45_364_441,
     "cone256": 6_962_229_058,
+    "batch64": 3_042_757_788,
 }
 METRIC = "GRays/s fwd+adj"
 L2_FLUSH_BYTES = 512 << 20
@@ -307,6 +308,7 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_launch": bytes_per_launch, "segments": seg, "kernels": kern}
 
     e2e = run_e2e(proj, x, y, args, dev, w) if args.e2e_steps > 0 else None
+    batched = run_batched(args, dev, flush) if (world == 1 and args.batched_steps > 0) else None
     cpu = None
     if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
         cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s)
@@ -320,7 +322,7 @@ def run_ours(args, world, rank, local):
                           "walk": ["auto", "lane", "column"][args.walk],
                           "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
                           "parallelism": f"independent scans x{world}"},
-               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+               "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "batched": batched,
                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(out))
 
@@ -365,6 +367,62 @@ def run_e2e(proj, x, y, args, dev, w):
             else "FanBeam2DProjector.__call__ + .back_project"}
 
 
+def run_batched(args, dev, flush):
+    """64 uneven 2-D scans (batch64): forward + adjoint of every scan in one
+    persistent launch each (autotuned tile shape), replayed from a CUDA graph,
+    against the per-scan loop of the same kernels.  Inputs resident, L2
+    flushed before every pass."""
+    from ct_laboratory_b200.batched import ScanBatch
+    from ct_laboratory_b200.workloads import WORKLOADS
+    w = WORKLOADS["batch64"]
+    t0 = time.perf_counter()
+    batch = ScanBatch(w.projectors(dev))
+    for img, ph in zip(batch.images_in, w.phantoms(device=dev)):
+        img.copy_(ph)
+    g = torch.Generator(device=dev).manual_seed(2)
+    for s in batch.sinos_in:
+        s.copy_(torch.rand(s.shape, generator=g, device=dev))
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cfg = batch.autotune(reps=3)
+    tune_s = time.perf_counter() - t0
+    graph = batch.capture()
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        for _ in range(args.batched_steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    with torch.no_grad():
+        ms_graph = timed(graph.replay)
+        ms_eager = timed(lambda: (batch.forward(), batch.back()))
+        ms_loop = timed(lambda: (batch.forward_loop(), batch.back_loop()))
+    n_ray = sum(int(p.src.shape[0]) for p in batch.projectors)
+    bytes_pair = 2 * (4 * SEGMENTS["batch64"] + 4 * n_ray)
+    peak, _ = peaks()
+    del graph
+    return {"workload": "batch64", "n_scan": len(batch.projectors), "n_ray": n_ray, "segments": SEGMENTS["batch64"],
+            "tile": {"block_threads": cfg["block_threads"], "kind": cfg["kind"], "n_cta": cfg["n_cta"]},
+            "ms_per_pass": {"graph": ms_graph, "batched": ms_eager, "per_scan_loop": ms_loop},
+            "grays_s": {"graph": n_ray / ms_graph / 1e6, "batched": n_ray / ms_eager / 1e6,
+                        "per_scan_loop": n_ray / ms_loop / 1e6},
+            "speedup_vs_loop": ms_loop / ms_graph, "gpu_launches_per_pass": {"graph": 3, "per_scan_loop": 128},
+            "roofline_frac": bytes_pair / (ms_graph / 1e3) / 1e9 / peak,
+            "setup_s": setup_s, "autotune_s": tune_s,
+            "note": "one pass = forward + adjoint of all 64 scans; L2 flushed before each pass; median of "
+                    f"{args.batched_steps}"}
+
+
 def load_traffic(workload, kernel):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -389,6 +447,8 @@ def main():
     ap.add_argument("--views", type=int, default=0,
                     help="override the workload's view count (smaller cases for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--batched-steps", type=int, default=10,
+                    help="timed passes of the 64-scan batched workload (0 = skip that leg)")
     ap.add_argument("--cpu-baseline-s", type=float, default=15.0)
     ap.add_argument("--ref-step-s", type=float, default=4.0)
     args = ap.parse_args()

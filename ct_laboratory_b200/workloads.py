@@ -7,12 +7,19 @@ cone256  3-D cone-beam: 256^3 volume, 0.5 mm voxels; 360 views over 360
 fan256   2-D fan-beam: 256^2 image, 1 mm pixels; 360 views; 512 bins at
          1 mm; SID 1000 mm, SDD 1500 mm; water disk + 10 seeded ellipses.
          184,320 rays ordered [view][bin].
+batch64  64 seeded 2-D scans of uneven size: image side uniform over
+         {128, 192, 256, 384, 512} (pixel = 256 mm / side, so every image
+         covers the same 256 mm field), views uniform over 90-720, half
+         fan-beam as fan256 (512 bins at 1 mm, SID 1000, SDD 1500), half
+         StaticCT rings: 16-64 sources on a 380 mm ring, 64 modules x 16
+         cells = 1024-cell arc detector on a 366.7 mm ring, views =
+         frames x sources with the gantry stepped between frames.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass
 
-__all__ = ["ConeWorkload", "FanWorkload", "WORKLOADS"]
+__all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "WORKLOADS"]
 
 
 @dataclass(frozen=True)
@@ -72,4 +79,67 @@ class FanWorkload:
         return ellipse_phantom_2d(*self.n, pixel=self.pixel, seed=self.seed, device=device)
 
 
-WORKLOADS = {"cone256": ConeWorkload(), "fan256": FanWorkload()}
+@dataclass(frozen=True)
+class ScanBatchWorkload:
+    name: str = "batch64"
+    n_scan: int = 64
+    sides: tuple = (128, 192, 256, 384, 512)
+    views: tuple = (90, 720)
+    sources: tuple = (16, 64)
+    fov: float = 256.0
+    seed: int = 0
+
+    def instances(self):
+        """One dict per scan: kind ('fan' / 'ring'), side, pixel, views and,
+        for rings, sources and frames."""
+        import numpy as np
+        rng = np.random.default_rng(self.seed)
+        out = []
+        for i in range(self.n_scan):
+            side = int(rng.choice(self.sides))
+            views = int(rng.integers(self.views[0], self.views[1] + 1))
+            d = {"kind": "fan" if i % 2 == 0 else "ring", "side": side, "pixel": self.fov / side, "views": views}
+            if d["kind"] == "ring":
+                n_source = int(rng.integers(self.sources[0], self.sources[1] + 1))
+                d["sources"] = n_source
+                d["frames"] = max(1, round(views / n_source))
+                d["views"] = d["sources"] * d["frames"]
+            out.append(d)
+        return out
+
+    def projectors(self, device):
+        """The scans' projector modules, built on the host (the ring builder
+        runs many small tensor operations) and moved to `device`."""
+        import math
+
+        import torch
+
+        from .tomography import FanBeam2DProjector, UniformStaticCTProjector2D, standard_image_transform_2d
+        out = []
+        for d in self.instances():
+            side, pixel = d["side"], d["pixel"]
+            if d["kind"] == "fan":
+                p = FanBeam2DProjector(side, side, n_view=d["views"], n_det=512, sid=1000.0, sdd=1500.0,
+                                       det_spacing=1.0, pixel_size=pixel, device=torch.device("cpu"))
+                out.append(p.to(device))
+                continue
+            n_source, n_frame = d["sources"], d["frames"]
+            step = 2 * math.pi / (n_source * n_frame)
+            Mg = torch.stack([torch.tensor([[math.cos(f * step), -math.sin(f * step)],
+                                            [math.sin(f * step), math.cos(f * step)]], dtype=torch.float32)
+                              for f in range(n_frame)])
+            bg = torch.zeros(n_frame, 2)
+            act = torch.ones(n_frame, n_source, dtype=torch.bool)
+            M, b = standard_image_transform_2d(side, side, pixel, pixel)
+            p = UniformStaticCTProjector2D(side, side, M, b, n_source, 380.0, 64, 366.7, 16,
+                                           2 * math.pi * 366.7 / 1024, Mg, bg, act, device=torch.device("cpu"))
+            out.append(p.to(device))
+        return out
+
+    def phantoms(self, device="cpu"):
+        from .phantoms import ellipse_phantom_2d
+        return [ellipse_phantom_2d(d["side"], d["side"], pixel=d["pixel"], seed=self.seed + 1 + i, device=device)
+                for i, d in enumerate(self.instances())]
+
+
+WORKLOADS = {"cone256": ConeWorkload(), "fan256": FanWorkload(), "batch64": ScanBatchWorkload()}
