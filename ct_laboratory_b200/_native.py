@@ -90,6 +90,7 @@ _SIGS = {
     "ctlab_forward_project_batched": [_BP, _I32, _P],
     "ctlab_back_project_batched": [_BP, _I, _I32, _P],
     "ctlab_batch_default_ctas": [_I32, _I, _I, _I32, ctypes.POINTER(_I32)],
+    "ctlab_project_batched_noalloc": [_SP, _I32, _I, _I, _I32, _I32, _P],
 }
 
 for _name, _args in _SIGS.items():

@@ -27,6 +27,7 @@
 // graph as long as the bound buffers stay where they are.
 #include "walk.cuh"
 
+#include <atomic>
 #include <vector>
 
 namespace ctlab {
@@ -361,4 +362,109 @@ extern "C" int ctlab_batch_default_ctas(int32_t ndim, int adjoint, int voxel_rul
     if (rc) return rc;
     *n_cta = v;
     return CTLAB_OK;
+}
+
+// ----------------------------------------------------------------------------
+// The batched projector for callers that cannot allocate device memory.
+//
+// Some programs that link this library must not call cudaMalloc: a plugin
+// inside a host application whose own allocator owns all of the GPU's memory
+// (a framework caching allocator, an inference server with a fixed memory
+// budget), or a real-time acquisition loop where an allocation could block
+// or fail in the middle of a scan.  ctlab_batch_plan asks such a caller for
+// a workspace it cannot provide; this entry point keeps the same scratch (the
+// work counter and the resolved scan table) in a fixed array that is part of
+// the library's own device image instead.
+// ----------------------------------------------------------------------------
+namespace ctlab {
+
+constexpr int kNoAllocMaxScans = 64;
+constexpr size_t kNoAllocBytes = sizeof(BatchHeader) + (size_t)kNoAllocMaxScans * sizeof(ScanDev);
+
+// Every GPU that loads the library holds this array (about 12.5 KB) until
+// the process exits.  Calls share it: it keeps the last call's table and
+// counter, so each call rewrites the table and clears the counter.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch per device.  In host code the array's
+// name is a host-side stand-in, not a device address, so the address is
+// looked up with cudaGetSymbolAddress, once per device with that device
+// current (the first call on each device), and cached.
+constexpr int kNoAllocMaxDevices = 64;
+static std::atomic<void*> g_noalloc_addr[kNoAllocMaxDevices];
+
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    CTLAB_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, "project_batched_noalloc: device %d beyond the %d supported",
+                  dev, kNoAllocMaxDevices);
+    void* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (p == nullptr) {
+        CTLAB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return CTLAB_OK;
+}
+
+}  // namespace ctlab
+
+extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_scan, int adjoint, int accumulate,
+                                             int32_t block_threads, int32_t n_cta, void* stream) {
+    clear_error();
+    const char* what = "project_batched_noalloc";
+    CTLAB_REQUIRE(scans != nullptr, "%s: null scans", what);
+    CTLAB_REQUIRE(n_scan >= 1 && n_scan <= kNoAllocMaxScans,
+                  "%s: n_scan must be in [1, %d], got %d (the library's fixed scratch holds at most %d scans; "
+                  "larger batches need ctlab_batch_plan with a caller-allocated workspace)",
+                  what, kNoAllocMaxScans, n_scan, kNoAllocMaxScans);
+    if (block_threads == 0) block_threads = 256;
+    CTLAB_REQUIRE(block_threads >= 32 && block_threads <= 256 && block_threads % 32 == 0,
+                  "%s: block_threads must be a multiple of 32 in [32, 256] (got %d)", what, block_threads);
+    CTLAB_REQUIRE(n_cta >= 0, "%s: n_cta must be >= 0 (0 = resident CTAs per SM x SMs)", what);
+    const int ndim = scans[0].ndim;
+    CTLAB_REQUIRE(ndim == 2 || ndim == 3, "%s: ndim must be 2 or 3 (got %d)", what, ndim);
+    const int rule = scans[0].opts.voxel_rule;
+    CTLAB_REQUIRE(rule == CTLAB_VOXEL_MIDPOINT || rule == CTLAB_VOXEL_CROSSING, "%s: unknown voxel_rule %d", what,
+                  rule);
+    ScanDev table[kNoAllocMaxScans];  // host stack, copied into the scratch below
+    int64_t tiles = 0;
+    for (int32_t i = 0; i < n_scan; ++i) {
+        int rc = resolve_scan(scans[i], i, ndim, block_threads, rule, table[i]);
+        if (rc) return rc;
+        const bool bound = adjoint ? scans[i].image_out != nullptr : scans[i].image_in != nullptr;
+        CTLAB_REQUIRE(bound, "%s: scan %d binds no %s buffers", what, i, adjoint ? "adjoint" : "forward");
+        table[i].first_tile = tiles;
+        tiles += table[i].T.n_blocks;
+        CTLAB_REQUIRE(tiles < kMaxBatchTiles, "%s: more than 2^31 tiles in one batch", what);
+    }
+    void* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    char* ws = static_cast<char*>(base);
+    const ScanDev* dtable = reinterpret_cast<const ScanDev*>(ws + sizeof(BatchHeader));
+    unsigned* counter = reinterpret_cast<unsigned*>(ws);
+    cudaStream_t s = as_stream(stream);
+    // From pageable (stack) memory: the copy waits for the stream's earlier
+    // work and has taken the table when it returns.
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(ws + sizeof(BatchHeader), table, sizeof(ScanDev) * (size_t)n_scan,
+                                   cudaMemcpyHostToDevice, s));
+    CTLAB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+    if (adjoint && !accumulate) {
+        batched_zero_kernel<<<dim3(64, (unsigned)n_scan), 256, 0, s>>>(dtable);
+        rc = launch_status(what);
+        if (rc) return rc;
+    }
+    if (tiles == 0) return CTLAB_OK;
+    const void* fn = pick_kernel(ndim, adjoint != 0, rule == CTLAB_VOXEL_MIDPOINT);
+    int ctas = n_cta;
+    if (ctas == 0) {
+        rc = default_ctas(fn, block_threads, &ctas);
+        if (rc) return rc;
+    }
+    const unsigned total = (unsigned)tiles;
+    int n = n_scan;
+    void* args[] = {(void*)&dtable, (void*)&n, (void*)&total, (void*)&counter};
+    CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)block_threads), args, 0, s));
+    return launch_status(what);
 }

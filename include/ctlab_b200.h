@@ -347,6 +347,33 @@ int ctlab_back_project_batched(const ctlab_batch* plan, int accumulate, int32_t 
  * of this kind (ndim, adjoint 0/1, voxel rule, block_threads). */
 int ctlab_batch_default_ctas(int32_t ndim, int adjoint, int voxel_rule, int32_t block_threads, int32_t* n_cta);
 
+/* The batched projector for callers that cannot allocate GPU memory: a
+ * plugin whose host application's allocator owns the whole device, or a
+ * real-time loop where an allocation could stall or fail mid-scan.  No
+ * counterpart in the reference (it has no batched or allocation-free path).
+ *
+ * Projects every scan of a host array once: the forward (adjoint = 0:
+ * sino_out = A image_in) or the adjoint (adjoint = 1: image_out = A^T sino_in,
+ * zeroed first unless accumulate = 1), with the results of
+ * ctlab_forward_project_batched / ctlab_back_project_batched.  The caller
+ * still owns every input and output buffer; the scratch those calls keep in
+ * a workspace (work counter, resolved scan table) lives instead in a fixed
+ * array inside the library's device image, of at most 64 scans (about
+ * 12.5 KB, held on every GPU that loads the library until the process
+ * exits).  More than 64 scans is rejected with CTLAB_EINVAL.  No cudaMalloc,
+ * cudaFree or other allocating call is made.
+ *
+ * The first call on each device looks up that array's device address (with
+ * the device current) and caches it; make that first call before any
+ * stream capture.  Each call copies the scan table in from host memory,
+ * which waits for work already queued on `stream`, and clears the work
+ * counter.  All calls share the one array, so calls whose work overlaps on
+ * the GPU (other streams, other host threads) race and give wrong results:
+ * issue them one after another.  block_threads (0 = 256) and n_cta
+ * (0 = resident CTAs per SM x SMs) as for the planned calls. */
+int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_scan, int adjoint, int accumulate,
+                                  int32_t block_threads, int32_t n_cta, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
