@@ -309,6 +309,7 @@ def run_ours(args, world, rank, local):
 
     e2e = run_e2e(proj, x, y, args, dev, w) if args.e2e_steps > 0 else None
     batched = run_batched(args, dev, flush) if (world == 1 and args.batched_steps > 0) else None
+    serving = run_serving(args, dev) if (world == 1 and args.serve_jobs > 0) else None
     cpu = None
     if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
         cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s)
@@ -323,6 +324,7 @@ def run_ours(args, world, rank, local):
                           "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
                           "parallelism": f"independent scans x{world}"},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "batched": batched,
+               "serving": serving,
                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(out))
 
@@ -423,6 +425,49 @@ def run_batched(args, dev, flush):
                     f"{args.batched_steps}"}
 
 
+def run_serving(args, dev):
+    """MAP reconstruction jobs arriving as a Poisson process (serve workload):
+    the plain per-job loop (reference-style estimator, one job at a time)
+    and the continuous-batching server on the same requests, back to back.
+    Latency = wall time from a job's arrival to its reconstruction on the
+    host; throughput = jobs / (last finish - first arrival)."""
+    import dataclasses
+
+    from ct_laboratory_b200.serving import ReconServer, latency_summary, make_jobs, sequential_baseline
+    from ct_laboratory_b200.workloads import WORKLOADS
+    w = dataclasses.replace(WORKLOADS["serve"], n_jobs=args.serve_jobs)
+    t0 = time.perf_counter()
+    jobs = make_jobs(w, dev)
+    make_s = time.perf_counter() - t0
+    plain = sequential_baseline(jobs, dev)
+    server_all = ReconServer(dev, policy="all")
+    sa = latency_summary(server_all.run(jobs))
+    server = ReconServer(dev, policy="srpt")
+    served = server.run(jobs)
+    ps, ss = latency_summary(plain), latency_summary(served)
+    xs = {r["job_id"]: r["x"] for r in served}
+    rel = []
+    for r in plain:
+        a, b = xs[r["job_id"]].double(), r["x"].double()
+        rel.append(float((a - b).norm() / b.norm().clamp_min(1e-30)))
+    mix = {}
+    for j in jobs:
+        mix[j.n] = mix.get(j.n, 0) + 1
+    return {"workload": "serve", "jobs": len(jobs), "arrival_rate_per_s": w.rate,
+            "mix": {f"{k}^3": v for k, v in sorted(mix.items())},
+            "rays_x_iters": sum(j.n_ray * j.iters for j in jobs),
+            "plain_loop": ps, "served": ss, "served_all_every_tick": sa,
+            "throughput_ratio": ss["jobs_per_s"] / ps["jobs_per_s"],
+            "p50_ratio": ss["p50_s"] / ps["p50_s"], "p99_ratio": ss["p99_s"] / ps["p99_s"],
+            "max_rel_rmse_served_vs_plain": max(rel),
+            "served_max_active": server.log[-1]["max_active"], "served_ticks": server.log[-1]["ticks"],
+            "request_build_s": make_s,
+            "note": "plain loop = ConeBeam3DProjector + MaximumAPosterioriEstimator per job in arrival order; "
+                    "served = ReconServer, policy srpt (admission by HBM budget; each tick one batched forward and "
+                    "adjoint launch over the active jobs with the least remaining work, >= 64M rays); "
+                    "served_all_every_tick = the same server advancing every active job each tick"}
+
+
 def load_traffic(workload, kernel):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -447,6 +492,8 @@ def main():
     ap.add_argument("--views", type=int, default=0,
                     help="override the workload's view count (smaller cases for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--serve-jobs", type=int, default=16,
+                    help="jobs of the MAP serving workload (0 = skip that leg)")
     ap.add_argument("--batched-steps", type=int, default=10,
                     help="timed passes of the 64-scan batched workload (0 = skip that leg)")
     ap.add_argument("--cpu-baseline-s", type=float, default=15.0)

@@ -11,6 +11,8 @@ allocates once:
   sinos_in[i]    adjoint input                    ([n_ray])
   images_out[i]  adjoint output                   (same shape as images_in[i])
 
+(or binds caller-owned tensors given as ``buffers={"images_in": [...], ...}``).
+
 ``forward()`` computes every sinos_out[i] = A_i images_in[i] in one launch
 of persistent CTAs that pull ray tiles of all scans from a device work
 counter (libctlab_b200.so ``ctlab_forward_project_batched``); ``back()`` the
@@ -106,7 +108,7 @@ def _cost(p):
 
 class ScanBatch:
     def __init__(self, projectors, voxel_rule=N.VOXEL_CROSSING, forward=True, adjoint=True, block_threads=256,
-                 kind="auto"):
+                 kind="auto", buffers=None):
         self.projectors = list(projectors)
         if not self.projectors:
             raise ValueError("ScanBatch needs at least one projector")
@@ -121,10 +123,27 @@ class ScanBatch:
         self.has_forward, self.has_adjoint = bool(forward), bool(adjoint)
         shapes = [_dims(p) for p in self.projectors]
         n_rays = [int(p.src.shape[0]) for p in self.projectors]
-        self.images_in = self._arena(shapes) if forward else None
-        self.sinos_out = self._arena([(n,) for n in n_rays]) if forward else None
-        self.sinos_in = self._arena([(n,) for n in n_rays]) if adjoint else None
-        self.images_out = self._arena(shapes) if adjoint else None
+        if buffers is None:
+            self.images_in = self._arena(shapes) if forward else None
+            self.sinos_out = self._arena([(n,) for n in n_rays]) if forward else None
+            self.sinos_in = self._arena([(n,) for n in n_rays]) if adjoint else None
+            self.images_out = self._arena(shapes) if adjoint else None
+        else:
+            # caller-owned tensors (e.g. the state of reconstruction jobs): one
+            # per scan, float32, contiguous, on the projectors' device
+            want = {"images_in": (forward, shapes), "sinos_out": (forward, [(n,) for n in n_rays]),
+                    "sinos_in": (adjoint, [(n,) for n in n_rays]), "images_out": (adjoint, shapes)}
+            for name, (used, shp) in want.items():
+                ts = buffers.get(name) if used else None
+                if used:
+                    if ts is None or len(ts) != len(shp):
+                        raise ValueError(f"ScanBatch: buffers['{name}'] needs one tensor per scan")
+                    for tt, s in zip(ts, shp):
+                        if (tt.dtype != torch.float32 or not tt.is_contiguous() or tt.device != self.device
+                                or tt.numel() != int(torch.Size(s).numel())):
+                            raise ValueError(f"ScanBatch: buffers['{name}'] must be contiguous float32 tensors of "
+                                             f"shape {tuple(s)} on {self.device}")
+                setattr(self, name, list(ts) if used else None)
         # heaviest rays first: long tiles start early, short ones fill the tail
         self.order = sorted(range(len(self.projectors)), key=lambda i: -_cost(self.projectors[i]))
         nbytes = N.lib.ctlab_batch_workspace_bytes(len(self.projectors))

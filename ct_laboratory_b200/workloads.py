@@ -14,12 +14,17 @@ batch64  64 seeded 2-D scans of uneven size: image side uniform over
          StaticCT rings: 16-64 sources on a 380 mm ring, 64 modules x 16
          cells = 1024-cell arc detector on a 366.7 mm ring, views =
          frames x sources with the gantry stepped between frames.
+serve    MAP reconstruction jobs arriving as a seeded Poisson process (mean
+         20 jobs/s): cone-beam volumes of 128^3 / 256^3 / 384^3 (probabilities
+         0.5 / 0.35 / 0.15) at 0.5 mm, 180-720 views of a 2n x 1.5n detector
+         at 0.8 mm (the cone256 proportions), 20-50 iterations, I0 log-uniform
+         over 1e4-1e6, quadratic smoothness prior weight 1e-2.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass
 
-__all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "WORKLOADS"]
+__all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "ServingWorkload", "WORKLOADS"]
 
 
 @dataclass(frozen=True)
@@ -142,4 +147,39 @@ class ScanBatchWorkload:
                 for i, d in enumerate(self.instances())]
 
 
-WORKLOADS = {"cone256": ConeWorkload(), "fan256": FanWorkload(), "batch64": ScanBatchWorkload()}
+@dataclass(frozen=True)
+class ServingWorkload:
+    """MAP reconstruction requests arriving as a seeded Poisson process."""
+    name: str = "serve"
+    n_jobs: int = 16
+    rate: float = 20.0
+    sizes: tuple = (128, 256, 384)
+    probs: tuple = (0.5, 0.35, 0.15)
+    views: tuple = (180, 720)
+    iters: tuple = (20, 50)
+    I0: tuple = (1e4, 1e6)
+    prior_w: float = 1e-2
+    voxel: float = 0.5
+    pitch: float = 0.8
+    seed: int = 0
+
+    def jobs(self):
+        """One dict per job (JobSpec fields; lr is set when the request is made)."""
+        import numpy as np
+        rng = np.random.default_rng(self.seed)
+        t = np.cumsum(rng.exponential(1.0 / self.rate, size=self.n_jobs))
+        t -= t[0]
+        out = []
+        for i in range(self.n_jobs):
+            n = int(rng.choice(self.sizes, p=self.probs))
+            out.append({"job_id": i, "arrival_s": float(t[i]), "n": n,
+                        "views": int(rng.integers(self.views[0], self.views[1] + 1)),
+                        "iters": int(rng.integers(self.iters[0], self.iters[1] + 1)),
+                        "I0": float(10 ** rng.uniform(np.log10(self.I0[0]), np.log10(self.I0[1]))),
+                        "lr": 0.0, "det_nx": 2 * n, "det_ny": 3 * n // 2, "voxel": self.voxel,
+                        "pitch": self.pitch, "prior_w": self.prior_w})
+        return out
+
+
+WORKLOADS = {"cone256": ConeWorkload(), "fan256": FanWorkload(), "batch64": ScanBatchWorkload(),
+             "serve": ServingWorkload()}

@@ -1,0 +1,91 @@
+"""Continuous-batching MAP serving (ReconServer) against the plain per-job
+loop through the reference-style API, alone-vs-mixed invariance, admission
+by HBM budget and mid-run joins.
+
+Tolerance: reconstructions within 1e-4 relative RMSE (the stated MAP bar)
+of the sequential MaximumAPosterioriEstimator run and of the same job
+served alone; the server's iteration is written out instead of autograd and
+its adjoint adds in a different atomic order, so results agree to float
+rounding, not bitwise."""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda")
+TOL = 1e-4
+
+
+def small_workload(**kw):
+    from ct_laboratory_b200.workloads import ServingWorkload
+    args = dict(n_jobs=5, rate=200.0, sizes=(24, 32, 40), probs=(0.4, 0.3, 0.3), views=(12, 30), iters=(5, 10),
+                I0=(1e4, 1e5), seed=3)
+    args.update(kw)
+    return ServingWorkload(**args)
+
+
+def rel_rmse(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def jobs():
+    from ct_laboratory_b200.serving import make_jobs
+    return make_jobs(small_workload(), DEV)
+
+
+def test_served_matches_sequential_estimator(jobs):
+    from ct_laboratory_b200.serving import ReconServer, sequential_baseline
+    served = {r["job_id"]: r for r in ReconServer(DEV).run(jobs)}
+    plain = {r["job_id"]: r for r in sequential_baseline(jobs, DEV)}
+    for j in jobs:
+        s, p = served[j.job_id], plain[j.job_id]
+        assert s["iters"] == p["iters"] == j.iters
+        assert float(p["x"].abs().max()) > 0
+        assert rel_rmse(s["x"], p["x"]) <= TOL, (j.job_id, rel_rmse(s["x"], p["x"]))
+
+
+def test_result_same_alone_and_in_the_mix(jobs):
+    from ct_laboratory_b200.serving import ReconServer
+    mixed = {r["job_id"]: r["x"] for r in ReconServer(DEV).run(jobs)}
+    for j in jobs:
+        alone = ReconServer(DEV).run([dataclasses.replace(j, arrival_s=0.0)])[0]["x"]
+        assert rel_rmse(mixed[j.job_id], alone) <= TOL, j.job_id
+
+
+def test_admission_respects_the_hbm_budget(jobs):
+    from ct_laboratory_b200.serving import ReconServer, job_bytes
+    big = sorted(job_bytes(j) for j in jobs)
+    budget = big[-1] + big[-2]  # room for the two largest at once, never three
+    server = ReconServer(DEV, budget_bytes=budget)
+    out = server.run([dataclasses.replace(j, arrival_s=0.0) for j in jobs])
+    assert len(out) == len(jobs) and all("x" in r for r in out)
+    assert 1 <= server.log[-1]["max_active"] <= 2
+    one = ReconServer(DEV, max_active=1)
+    one.run(jobs)
+    assert one.log[-1]["max_active"] == 1
+
+
+def test_late_arrival_joins_running_jobs(jobs):
+    from ct_laboratory_b200.serving import ReconServer
+    early = dataclasses.replace(jobs[0], arrival_s=0.0, iters=3000)
+    late = dataclasses.replace(jobs[1], arrival_s=0.002)
+    for policy in ("all", "srpt"):
+        server = ReconServer(DEV, policy=policy)
+        res = {r["job_id"]: r for r in server.run([early, late])}
+        # the late job is admitted while the early one is still iterating
+        assert res[late.job_id]["admit_s"] < res[early.job_id]["finish_s"], policy
+        assert server.log[-1]["max_active"] == 2
+        if policy == "srpt":  # the short late job overtakes the long one
+            assert res[late.job_id]["finish_s"] < res[early.job_id]["finish_s"]
+
+
+def test_srpt_and_all_policies_give_the_same_reconstructions(jobs):
+    from ct_laboratory_b200.serving import ReconServer
+    a = {r["job_id"]: r["x"] for r in ReconServer(DEV, policy="all").run(jobs)}
+    b = {r["job_id"]: r["x"] for r in ReconServer(DEV, policy="srpt", tick_rays=1).run(jobs)}
+    for j in jobs:
+        assert rel_rmse(a[j.job_id], b[j.job_id]) <= TOL

@@ -1,0 +1,35 @@
+"""Host-side logic that needs no GPU: workload generators (seeded, shapes
+and ranges as specified) and the serving bookkeeping."""
+from ct_laboratory_b200.serving import JobSpec, job_bytes, latency_summary
+from ct_laboratory_b200.workloads import WORKLOADS
+
+
+def test_serving_workload_is_seeded_and_in_range():
+    w = WORKLOADS["serve"]
+    a, b = w.jobs(), w.jobs()
+    assert a == b and len(a) == w.n_jobs
+    arr = [d["arrival_s"] for d in a]
+    assert arr[0] == 0.0 and arr == sorted(arr)
+    for d in a:
+        assert d["n"] in w.sizes and w.views[0] <= d["views"] <= w.views[1] and w.iters[0] <= d["iters"] <= w.iters[1]
+        assert w.I0[0] <= d["I0"] <= w.I0[1] and d["det_nx"] == 2 * d["n"] and d["det_ny"] == 3 * d["n"] // 2
+
+
+def test_job_footprint_and_latency_summary():
+    s = JobSpec(**WORKLOADS["serve"].jobs()[0])
+    assert job_bytes(s) == 36 * s.n_ray + 16 * s.n ** 3
+    summ = latency_summary([{"latency_s": 1.0, "arrival_s": 0.0, "finish_s": 1.0},
+                            {"latency_s": 3.0, "arrival_s": 1.0, "finish_s": 4.0}])
+    assert summ["jobs"] == 2 and abs(summ["jobs_per_s"] - 0.5) < 1e-12 and summ["p50_s"] == 2.0
+
+
+def test_batch_workload_is_seeded_and_in_range():
+    w = WORKLOADS["batch64"]
+    ins = w.instances()
+    assert ins == w.instances() and len(ins) == 64
+    for d in ins:
+        assert d["side"] in w.sides and abs(d["pixel"] * d["side"] - w.fov) < 1e-9
+        if d["kind"] == "ring":
+            assert w.sources[0] <= d["sources"] <= w.sources[1] and d["views"] == d["sources"] * d["frames"]
+        else:
+            assert w.views[0] <= d["views"] <= w.views[1]
