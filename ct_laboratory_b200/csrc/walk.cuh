@@ -413,7 +413,12 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
 // ----------------------------------------------------------------------------
 constexpr unsigned kFullMask = 0xffffffffu;
 constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
-constexpr int kGroup = 4;   // cells walked per inner step (kChunk is a multiple)
+// Cells walked per inner step (both divide kChunk): the forward issues the
+// gathers of 8 cells together (up to 16 loads in flight per lane), the
+// adjoint's reductions need no results and walk 4 at a time (measured
+// fastest for each on the cone-beam benchmark scan).
+constexpr int kGroupFwd = 8;
+constexpr int kGroupAdj = 4;
 
 struct XYCell {
     float t;  // parameter of the crossing that ends the cell
@@ -498,27 +503,32 @@ struct ZWalk {
     int kz, dsz;
 };
 
-// kGroup cells of the buffer from position q: segment A = [t_cur, ts] in
-// (column, k), segment B = [ts, te] in (column, k') after a z step.
+// NG cells of the buffer from position q: segment A = [t_cur, ts] in
+// (column, k), segment B = [ts, te] in (column, k') after a z step.  With
+// LEN the segments are lengths (t1 - t0) * |v| (the reference's formula,
+// ct_projector_3d.cu:998); without, parameter spans t1 - t0 that the caller
+// scales by |v| itself.
+template <int NG>
 struct CellGroup {
-    float sa[kGroup], sb[kGroup];
-    unsigned ia[kGroup], ib[kGroup];  // voxel indices, valid where the segment is positive
+    float sa[NG], sb[NG];
+    unsigned ia[NG], ib[NG];  // voxel indices, valid where the segment is positive
 };
 
-__device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup& g, ZWalk& Z) {
+template <int NG, bool LEN>
+__device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup<NG>& g, ZWalk& Z) {
 #pragma unroll
-    for (int u = 0; u < kGroup; ++u) {
+    for (int u = 0; u < NG; ++u) {
         const XYCell c = buf[q + u];
         const float te = fminf(c.t, Z.t_end);
         const float ts = fminf(Z.tnz, te);
-        g.sa[u] = __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len);
+        g.sa[u] = LEN ? __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len) : __fsub_rn(ts, Z.t_cur);
         g.ia[u] = (unsigned)(c.col + Z.kz);
         if (Z.tnz <= te) {  // a z plane inside the cell (or ending it)
             Z.kz += Z.dsz;
             Z.pnz += Z.psz;
             Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
         }
-        g.sb[u] = __fmul_rn(__fsub_rn(te, ts), Z.len);
+        g.sb[u] = LEN ? __fmul_rn(__fsub_rn(te, ts), Z.len) : __fsub_rn(te, ts);
         g.ib[u] = (unsigned)(c.col + Z.kz);
         Z.t_cur = fmaxf(Z.t_cur, te);
     }
@@ -527,19 +537,21 @@ __device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup& 
 // A positive segment lies inside the lane's [t_enter, t_exit] and between
 // crossed planes only, so its voxel is inside the grid; zero-length ones
 // (before entry, after exit, ties) are neither read nor added.
-__device__ __forceinline__ void gather_group(const float* vol, const CellGroup& g, float* v, uint64_t pol) {
+template <int NG>
+__device__ __forceinline__ void gather_group(const float* vol, const CellGroup<NG>& g, float* v, uint64_t pol) {
 #pragma unroll
-    for (int u = 0; u < kGroup; ++u) {
+    for (int u = 0; u < NG; ++u) {
         if (g.sa[u] > 0.f) v[u] = ld_keep(vol + g.ia[u], pol);
-        if (g.sb[u] > 0.f) v[kGroup + u] = ld_keep(vol + g.ib[u], pol);
+        if (g.sb[u] > 0.f) v[NG + u] = ld_keep(vol + g.ib[u], pol);
     }
 }
 
-__device__ __forceinline__ float accumulate_group(const CellGroup& g, const float* v, float acc) {
+template <int NG>
+__device__ __forceinline__ float accumulate_group(const CellGroup<NG>& g, const float* v, float acc) {
 #pragma unroll
-    for (int u = 0; u < kGroup; ++u) {
+    for (int u = 0; u < NG; ++u) {
         if (g.sa[u] > 0.f) acc = __fmaf_rn(v[u], g.sa[u], acc);
-        if (g.sb[u] > 0.f) acc = __fmaf_rn(v[kGroup + u], g.sb[u], acc);
+        if (g.sb[u] > 0.f) acc = __fmaf_rn(v[NG + u], g.sb[u], acc);
     }
     return acc;
 }
@@ -669,6 +681,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     const uint64_t pol = l2_policy_keep();
     const float fl = (float)lane;
     const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
+    const float yl = __fmul_rn(y, Z.len);  // adjoint: y * |v| (0 on dead lanes)
 #pragma unroll 1
     for (int round = 0; round < max_rounds; ++round) {
         // lane l: the l-th next x plane and the l-th next y plane (plane
@@ -686,26 +699,28 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
         const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
         const int n_cells = min(n_in + 1, kChunk);
         if constexpr (ADJ) {
+            // y * |v| once per lane, times each parameter span: the same
+            // segment lengths as the forward's, multiplied in another order
 #pragma unroll 1
-            for (int q = 0; q < n_cells; q += kGroup) {
-                CellGroup g;
-                walk_group(buf, q, g, Z);
+            for (int q = 0; q < n_cells; q += kGroupAdj) {
+                CellGroup<kGroupAdj> g;
+                walk_group<kGroupAdj, false>(buf, q, g, Z);
 #pragma unroll
-                for (int u = 0; u < kGroup; ++u) {
-                    red_add_if(vout + g.ia[u], __fmul_rn(y, g.sa[u]), g.sa[u] > 0.f);
-                    red_add_if(vout + g.ib[u], __fmul_rn(y, g.sb[u]), g.sb[u] > 0.f);
+                for (int u = 0; u < kGroupAdj; ++u) {
+                    red_add_if(vout + g.ia[u], __fmul_rn(yl, g.sa[u]), g.sa[u] > 0.f);
+                    red_add_if(vout + g.ib[u], __fmul_rn(yl, g.sb[u]), g.sb[u] > 0.f);
                 }
             }
         } else {
-            // the group's gathers are issued together (up to 2 * kGroup in
+            // the group's gathers are issued together (up to 2 * kGroupFwd in
             // flight), then accumulated in walk order
 #pragma unroll 1
-            for (int q = 0; q < n_cells; q += kGroup) {
-                CellGroup g;
-                float v[2 * kGroup];
-                walk_group(buf, q, g, Z);
-                gather_group(vol, g, v, pol);
-                acc = accumulate_group(g, v, acc);
+            for (int q = 0; q < n_cells; q += kGroupFwd) {
+                CellGroup<kGroupFwd> g;
+                float v[2 * kGroupFwd];
+                walk_group<kGroupFwd, true>(buf, q, g, Z);
+                gather_group<kGroupFwd>(vol, g, v, pol);
+                acc = accumulate_group<kGroupFwd>(g, v, acc);
             }
         }
         if (n_in < kChunk) break;
