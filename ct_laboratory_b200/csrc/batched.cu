@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
             if constexpr (MID) {
                 if (r >= 0) lane_ray<3, ADJ, true>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
             } else {
-                shared_xy_ray<ADJ>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0, buf);
+                shared_xy_ray<ADJ, 1>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0, 1, buf);
             }
         } else {
             const Affine2 A = load_affine2(S->M_inv, S->b);

@@ -27,17 +27,18 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
 #define CTLAB_XY_MIN_BLOCKS 4
 #endif
 
-template <bool ADJ>
-__global__ void __launch_bounds__(256, CTLAB_XY_MIN_BLOCKS) siddon3d_shared_xy_kernel(const float* __restrict__ in,
-                                                                 float* __restrict__ out,
-                                                                 const float* __restrict__ src,
-                                                                 const float* __restrict__ dst, int64_t n_ray,
-                                                                 const float* __restrict__ M_inv,
-                                                                 const float* __restrict__ bvec, GridDims<3> G,
-                                                                 int64_t nvox, Tiling T) {
+// blockIdx.y covers batch items NB at a time: the walk of a tile is done once
+// for NB volumes (a batch of B volumes costs B / NB walks, not B).
+template <bool ADJ, int NB>
+__global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
+    siddon3d_shared_xy_kernel(const float* __restrict__ in, float* __restrict__ out, const float* __restrict__ src,
+                              const float* __restrict__ dst, int64_t n_ray, const float* __restrict__ M_inv,
+                              const float* __restrict__ bvec, GridDims<3> G, int64_t nvox, Tiling T, int batch) {
     __shared__ XYCell cells[256 / 32][kChunk];
     const Affine3 A = load_affine3(M_inv, bvec);
-    shared_xy_ray<ADJ>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), blockIdx.y, cells[threadIdx.x >> 5]);
+    const int64_t b0 = (int64_t)blockIdx.y * NB;
+    const int nb = min(NB, batch - (int)b0);
+    shared_xy_ray<ADJ, NB>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), b0, nb, cells[threadIdx.x >> 5]);
 }
 
 
@@ -92,7 +93,15 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
         const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
         if (!flat && !mid && small_grid && T.tile_rows % 32 == 0 &&
             (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
-            siddon3d_shared_xy_kernel<ADJ><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+            const int nb = batch >= 4 ? 4 : (batch >= 2 ? 2 : 1);
+            const dim3 g((unsigned)T.n_blocks, (unsigned)((batch + nb - 1) / nb));
+            const int bt = (int)batch;
+            if (nb == 4)
+                siddon3d_shared_xy_kernel<ADJ, 4><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+            else if (nb == 2)
+                siddon3d_shared_xy_kernel<ADJ, 2><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+            else
+                siddon3d_shared_xy_kernel<ADJ, 1><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
             return launch_status(what);
         }
     }

@@ -556,15 +556,17 @@ __device__ __forceinline__ float accumulate_group(const CellGroup<NG>& g, const 
     return acc;
 }
 
-// Per-thread body of the shared x-y walk: ray r of batch item bi (r = -1: the
-// thread has no ray but still takes part in the warp's collective steps).
-// All 32 lanes of the warp call it together; `buf` is the warp's kChunk-entry
-// shared-memory cell buffer.
-template <bool ADJ>
+// Per-thread body of the shared x-y walk for ray r (r = -1: the thread has no
+// ray but still takes part in the warp's collective steps) and the nb <= NB
+// batch items b0 .. b0+nb-1: the walk is done once and every segment gathers
+// from (forward) or reduces into (adjoint) all nb volumes.  All 32 lanes of
+// the warp call it together; `buf` is the warp's kChunk-entry shared-memory
+// cell buffer.
+template <bool ADJ, int NB>
 __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, float* __restrict__ out,
                                               const float* __restrict__ src, const float* __restrict__ dst,
                                               int64_t n_ray, const Affine3& A, const GridDims<3>& G,
-                                              int64_t nvox, int64_t r, int64_t bi, XYCell* buf) {
+                                              int64_t nvox, int64_t r, int64_t b0, int nb, XYCell* buf) {
     const int lane = threadIdx.x & 31;
     float sw[3] = {0.f, 0.f, 0.f}, dw[3] = {0.f, 0.f, 0.f};
     if (r >= 0) {
@@ -574,17 +576,27 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
             dw[a] = ld_stream(dst + r * 3 + a);
         }
     }
-    float y = 0.f;
-    if constexpr (ADJ) {
-        if (r >= 0) y = ld_stream(in + bi * n_ray + r);
+    float y[NB];
+    bool any_y = false;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        y[j] = 0.f;
+        if constexpr (ADJ) {
+            if (r >= 0 && j < nb) y[j] = ld_stream(in + (b0 + j) * n_ray + r);
+        }
+        any_y = any_y || y[j] != 0.f;
     }
     LaneRay R;
     lane_setup(R, sw, dw, G, A);
-    R.live = R.live && (r >= 0) && (!ADJ || y != 0.f);
+    R.live = R.live && (r >= 0) && (!ADJ || any_y);
 
     const unsigned live_mask = __ballot_sync(kFullMask, R.live);
     if (live_mask == 0u) {
-        if (!ADJ && r >= 0) st_stream(out + bi * n_ray + r, 0.f);
+        if (!ADJ && r >= 0) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, 0.f);
+        }
         return;
     }
     // Do the live lanes share their x-y line, and is every live lane's z
@@ -602,12 +614,18 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
                                 fabsf(R.s[1]) <= 131072.f && fabsf(R.s[2]) <= 131072.f);
     if (!__all_sync(kFullMask, ok) || vxy == 0.f) {
         if (r < 0) return;
-        if constexpr (ADJ) {
-            if (R.live) traverse<3, true, false>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
-        } else {
-            st_stream(out + bi * n_ray + r,
-                      R.live ? traverse<3, false, false>(in + bi * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
-                             : 0.f);
+#pragma unroll 1
+        for (int j = 0; j < nb; ++j) {  // the per-lane walk, once per volume
+            const int64_t b = b0 + j;
+            if constexpr (ADJ) {
+                const float yj = ld_stream(in + b * n_ray + r);
+                if (R.live && yj != 0.f)
+                    traverse<3, true, false>(nullptr, out + b * nvox, yj, sw, dw, G, A, (unsigned)nvox);
+            } else {
+                st_stream(out + b * n_ray + r,
+                          R.live ? traverse<3, false, false>(in + b * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
+                                 : 0.f);
+            }
         }
         return;
     }
@@ -674,14 +692,25 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     // ---- rounds of 32 x-y crossings ---------------------------------------
     // Each round consumes 32 crossings of the x-y sequence; after
     // n_x + n_y + 2 of them both exit planes lie behind, so the bound below
-    // is never the reason the loop ends.
-    const float* __restrict__ vol = ADJ ? nullptr : pin_ptr(in + bi * nvox);
-    float* __restrict__ vout = ADJ ? pin_ptr(out + bi * nvox) : nullptr;
-    float acc = 0.f;
+    // is never the reason the loop ends.  Volumes past nb alias the last
+    // valid one (their results are not stored, their reductions predicated
+    // off), so every address stays inside the batch.
+    const float* vol[NB];
+    float* vout[NB];
+    float acc[NB], yl[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        const int64_t b = b0 + (j < nb ? j : nb - 1);
+        vol[j] = ADJ ? nullptr : pin_ptr(in + b * nvox);
+        vout[j] = ADJ ? pin_ptr(out + b * nvox) : nullptr;
+        acc[j] = 0.f;
+        yl[j] = __fmul_rn(y[j], Z.len);  // adjoint: y * |v| (0 on dead lanes)
+    }
     const uint64_t pol = l2_policy_keep();
     const float fl = (float)lane;
     const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
-    const float yl = __fmul_rn(y, Z.len);  // adjoint: y * |v| (0 on dead lanes)
+    // forward: cells per step so that every step has 2 * kGroupFwd gathers in flight
+    constexpr int kGF = kGroupFwd / NB > 0 ? kGroupFwd / NB : 1;
 #pragma unroll 1
     for (int round = 0; round < max_rounds; ++round) {
         // lane l: the l-th next x plane and the l-th next y plane (plane
@@ -706,21 +735,26 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
                 CellGroup<kGroupAdj> g;
                 walk_group<kGroupAdj, false>(buf, q, g, Z);
 #pragma unroll
-                for (int u = 0; u < kGroupAdj; ++u) {
-                    red_add_if(vout + g.ia[u], __fmul_rn(yl, g.sa[u]), g.sa[u] > 0.f);
-                    red_add_if(vout + g.ib[u], __fmul_rn(yl, g.sb[u]), g.sb[u] > 0.f);
+                for (int j = 0; j < NB; ++j) {
+#pragma unroll
+                    for (int u = 0; u < kGroupAdj; ++u) {
+                        red_add_if(vout[j] + g.ia[u], __fmul_rn(yl[j], g.sa[u]), g.sa[u] > 0.f && j < nb);
+                        red_add_if(vout[j] + g.ib[u], __fmul_rn(yl[j], g.sb[u]), g.sb[u] > 0.f && j < nb);
+                    }
                 }
             }
         } else {
-            // the group's gathers are issued together (up to 2 * kGroupFwd in
-            // flight), then accumulated in walk order
+            // the step's gathers are issued together, then accumulated in
+            // walk order, volume by volume
 #pragma unroll 1
-            for (int q = 0; q < n_cells; q += kGroupFwd) {
-                CellGroup<kGroupFwd> g;
-                float v[2 * kGroupFwd];
-                walk_group<kGroupFwd, true>(buf, q, g, Z);
-                gather_group<kGroupFwd>(vol, g, v, pol);
-                acc = accumulate_group<kGroupFwd>(g, v, acc);
+            for (int q = 0; q < n_cells; q += kGF) {
+                CellGroup<kGF> g;
+                walk_group<kGF, true>(buf, q, g, Z);
+                float v[NB][2 * kGF];
+#pragma unroll
+                for (int j = 0; j < NB; ++j) gather_group<kGF>(vol[j], g, v[j], pol);
+#pragma unroll
+                for (int j = 0; j < NB; ++j) acc[j] = accumulate_group<kGF>(g, v[j], acc[j]);
             }
         }
         if (n_in < kChunk) break;
@@ -730,9 +764,12 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
         pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
     }
     if constexpr (!ADJ) {
-        if (r >= 0) st_stream(out + bi * n_ray + r, acc);
+        if (r >= 0) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, acc[j]);
+        }
     }
 }
-
 
 }  // namespace ctlab
