@@ -337,20 +337,38 @@ def _fwd3(proj, x):
 
 def run_e2e(proj, x, y, args, dev, w):
     """Public API, host buffers: H2D of the volume and of the adjoint input,
-    D2H of the sinogram and of the back-projection, every step."""
+    D2H of the sinogram and of the back-projection, every step.  The copies
+    run on a second stream so that the adjoint input's H2D proceeds under the
+    forward and the sinogram's D2H under the adjoint; the timed region ends
+    when every copy of the last step has landed."""
     x_h = x.cpu().pin_memory()
     y_h = y.cpu().pin_memory()
     sino_h = torch.empty(y.shape, dtype=torch.float32).pin_memory()
     vol_h = torch.empty(x.shape, dtype=torch.float32).pin_memory()
+    xd, yd = torch.empty_like(x), torch.empty_like(y)
     stream = torch.cuda.current_stream(dev)
+    copy = torch.cuda.Stream(dev)
 
     def step():
-        xd = x_h.to(dev, non_blocking=True)
+        copy.wait_stream(stream)  # the previous step is done with xd / yd
+        with torch.cuda.stream(copy):
+            xd.copy_(x_h, non_blocking=True)
+            ev_x = copy.record_event()
+            yd.copy_(y_h, non_blocking=True)
+            ev_y = copy.record_event()
+        stream.wait_event(ev_x)
         s = proj(xd)
-        sino_h.copy_(s, non_blocking=True)
-        yd = y_h.to(dev, non_blocking=True)
+        ev_f = stream.record_event()
+        stream.wait_event(ev_y)
         v = proj.back_project(yd)
-        vol_h.copy_(v, non_blocking=True)
+        ev_b = stream.record_event()
+        with torch.cuda.stream(copy):
+            copy.wait_event(ev_f)
+            sino_h.copy_(s, non_blocking=True)
+            s.record_stream(copy)
+            copy.wait_event(ev_b)
+            vol_h.copy_(v, non_blocking=True)
+            v.record_stream(copy)
 
     with torch.no_grad():
         for _ in range(2):
@@ -360,6 +378,7 @@ def run_e2e(proj, x, y, args, dev, w):
         e0.record(stream)
         for _ in range(args.e2e_steps):
             step()
+        stream.wait_stream(copy)
         e1.record(stream)
         torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / args.e2e_steps
@@ -367,8 +386,8 @@ def run_e2e(proj, x, y, args, dev, w):
     return {"value": n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
             "h2d_bytes_per_step": int(x_h.numel() * 4 + y_h.numel() * 4),
             "d2h_bytes_per_step": int(sino_h.numel() * 4 + vol_h.numel() * 4),
-            "api": "ConeBeam3DProjector.__call__ + .back_project" if w.name.startswith("cone")
-            else "FanBeam2DProjector.__call__ + .back_project"}
+            "api": ("ConeBeam3DProjector.__call__ + .back_project" if w.name.startswith("cone")
+                    else "FanBeam2DProjector.__call__ + .back_project") + ", copies on a second stream"}
 
 
 def run_batched(args, dev, flush):
@@ -416,7 +435,8 @@ def run_batched(args, dev, flush):
     peak, _ = peaks()
     del graph
     return {"workload": "batch64", "n_scan": len(batch.projectors), "n_ray": n_ray, "segments": SEGMENTS["batch64"],
-            "tile": {"block_threads": cfg["block_threads"], "kind": cfg["kind"], "n_cta": cfg["n_cta"]},
+            "tile": {"forward": {k: cfg[k] for k in ("block_threads", "kind", "n_cta")},
+                     "adjoint": {k: batch.config_adj[k] for k in ("block_threads", "kind", "n_cta")}},
             "ms_per_pass": {"graph": ms_graph, "batched": ms_eager, "per_scan_loop": ms_loop},
             "grays_s": {"graph": n_ray / ms_graph / 1e6, "batched": n_ray / ms_eager / 1e6,
                         "per_scan_loop": n_ray / ms_loop / 1e6},

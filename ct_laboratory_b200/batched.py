@@ -70,8 +70,14 @@ def tile_kinds(p):
     """Tile layouts that apply to projector p (the autotuner's choices).
 
     flat      consecutive rays, block_threads per CTA
-    grid32    2-D: 32 detector cells x (block_threads/32) views per CTA
+    grid32    2-D: 32 detector cells x (block_threads/32) views per CTA, lanes
+              along cells (neighbouring rays: coherent gathers, the forward's
+              choice)
     grid64    2-D: 64 cells x (block_threads/64) views
+    vgrid32   2-D: 32 views x (block_threads/32) cells, lanes along views (the
+              same cell seen from 32 directions: the lanes' pixels are far
+              apart, so the adjoint's reductions do not collide)
+    vgrid64   2-D: 64 views x (block_threads/64) cells
     col32     3-D detector grid: 32 detector rows x (block_threads/32) columns
               (lanes of a warp down one detector column: the column walk)
     col64     3-D: 64 rows x (block_threads/64) columns
@@ -79,7 +85,7 @@ def tile_kinds(p):
     kinds = ["flat"]
     if _ndim(p) == 2:
         if _ray_grid(p) is not None:
-            kinds += ["grid32", "grid64"]
+            kinds += ["grid32", "grid64", "vgrid32", "vgrid64"]
     elif getattr(p, "ray_tiling", None) is not None and p.ray_tiling.n_view > 0:
         kinds += ["col32", "col64"]
     return kinds
@@ -88,13 +94,18 @@ def tile_kinds(p):
 def _opts(p, kind, voxel_rule, block_threads):
     """RayOpts of projector p laid out as `kind` (falls back to flat when the
     kind does not apply or does not fit block_threads)."""
-    rows = {"grid32": 32, "grid64": 64, "col32": 32, "col64": 64}.get(kind)
+    rows = {"grid32": 32, "grid64": 64, "vgrid32": 32, "vgrid64": 64, "col32": 32, "col64": 64}.get(kind)
     if rows is None or rows > block_threads or kind not in tile_kinds(p):
         return N.flat_opts(voxel_rule=voxel_rule, block_threads=block_threads)
     if kind.startswith("grid"):
         n_view, n_bin = _ray_grid(p)
         # rows = detector cells (stride 1), columns = views (stride n_bin)
         return N.tiling(1, n_bin, n_view, n_bin * n_view, 1, n_bin, tile_rows=rows, block_threads=block_threads,
+                        voxel_rule=voxel_rule)
+    if kind.startswith("vgrid"):
+        n_view, n_bin = _ray_grid(p)
+        # rows = views (stride n_bin), columns = detector cells (stride 1)
+        return N.tiling(1, n_view, n_bin, n_bin * n_view, n_bin, 1, tile_rows=rows, block_threads=block_threads,
                         voxel_rule=voxel_rule)
     t = p.ray_tiling
     return N.tiling(t.n_view, t.n_row, t.n_col, t.view_stride, t.row_stride, t.col_stride, tile_rows=rows,
@@ -149,12 +160,16 @@ class ScanBatch:
         nbytes = N.lib.ctlab_batch_workspace_bytes(len(self.projectors))
         if nbytes < 0:
             raise ValueError(f"ScanBatch: {len(self.projectors)} scans is outside [1, 65535]")
-        self._ws = torch.empty(int(nbytes) + 256, dtype=torch.uint8, device=self.device)
-        off = (-self._ws.data_ptr()) % 256
-        self._ws_ptr = self._ws.data_ptr() + off
+        # one plan (and workspace) per direction: the forward and the adjoint
+        # may lay their tiles out differently
         self._ws_bytes = int(nbytes)
-        self._plan = N.Batch()
+        self._ws, self._ws_ptr, self._plans = {}, {}, {}
+        for d in ("fwd", "adj"):
+            self._ws[d] = torch.empty(self._ws_bytes + 256, dtype=torch.uint8, device=self.device)
+            self._ws_ptr[d] = self._ws[d].data_ptr() + (-self._ws[d].data_ptr()) % 256
+            self._plans[d] = N.Batch()
         self.config = None
+        self.config_adj = None
         self.configure(block_threads=block_threads, kind=kind)
 
     # ------------------------------------------------------------ buffers
@@ -189,50 +204,73 @@ class ScanBatch:
         s.opts = _opts(p, k, self.voxel_rule, block_threads)
         return s
 
-    def configure(self, block_threads=256, kind="auto", n_cta=0):
+    def _default_kinds(self, direction):
+        out = []
+        for p in self.projectors:
+            k = tile_kinds(p)
+            if "col32" in k:
+                out.append("col32")
+            elif direction == "adj" and "vgrid32" in k:
+                out.append("vgrid32")
+            elif "grid32" in k:
+                out.append("grid32")
+            else:
+                out.append("flat")
+        return out
+
+    def configure(self, block_threads=256, kind="auto", n_cta=0, direction="both"):
         """(Re)plan the batch with a tile layout: `kind` is one tile kind for
-        every scan (the first that applies when it is "auto": col32 / grid32 /
-        flat) or a list with one kind per scan."""
-        if kind == "auto":
-            kind = ["col32" if "col32" in tile_kinds(p) else "flat" for p in self.projectors]
-        arr = (N.Scan * len(self.projectors))(*[self._scan(i, kind, block_threads) for i in self.order])
-        with torch.cuda.device(self.device):
-            N.call("ctlab_batch_plan", arr, len(self.projectors), int(block_threads), ctypes.c_void_p(self._ws_ptr),
-                   self._ws_bytes, ctypes.byref(self._plan), N.stream_of(self._ws))
-            if n_cta == 0:
-                v = ctypes.c_int32(0)
-                N.call("ctlab_batch_default_ctas", self.ndim, int(self.has_adjoint and not self.has_forward),
-                       self.voxel_rule, int(block_threads), ctypes.byref(v))
-                n_cta = v.value
-        self.config = {"block_threads": int(block_threads), "kind": kind, "n_cta": int(n_cta)}
-        self._loop_opts = [_opts(self.projectors[i], kind if isinstance(kind, str) else kind[i], self.voxel_rule,
-                                 block_threads) for i in range(len(self.projectors))]
+        every scan or a list with one kind per scan; "auto" takes col32 for
+        detector grids in 3-D, grid32 (forward) / vgrid32 (adjoint) for 2-D
+        view x cell grids, else flat.  `direction` ("fwd", "adj" or "both")
+        selects the plan(s) to replace.  Returns the forward configuration
+        (the adjoint's is ``config_adj``)."""
+        for d in (("fwd", "adj") if direction == "both" else (direction,)):
+            k = self._default_kinds(d) if kind == "auto" else kind
+            arr = (N.Scan * len(self.projectors))(*[self._scan(i, k, block_threads) for i in self.order])
+            with torch.cuda.device(self.device):
+                N.call("ctlab_batch_plan", arr, len(self.projectors), int(block_threads),
+                       ctypes.c_void_p(self._ws_ptr[d]), self._ws_bytes, ctypes.byref(self._plans[d]),
+                       N.stream_of(self._ws[d]))
+                ctas = n_cta
+                if ctas == 0:
+                    v = ctypes.c_int32(0)
+                    N.call("ctlab_batch_default_ctas", self.ndim, int(d == "adj"), self.voxel_rule,
+                           int(block_threads), ctypes.byref(v))
+                    ctas = v.value
+            cfg = {"block_threads": int(block_threads), "kind": k, "n_cta": int(ctas)}
+            opts = [_opts(self.projectors[i], k if isinstance(k, str) else k[i], self.voxel_rule, block_threads)
+                    for i in range(len(self.projectors))]
+            if d == "fwd":
+                self.config, self._loop_opts_f = cfg, opts
+            else:
+                self.config_adj, self._loop_opts_a = cfg, opts
         return self.config
 
     @property
     def total_tiles(self):
-        return int(self._plan.total_tiles)
+        return int(self._plans["fwd"].total_tiles)
 
     # ------------------------------------------------------------ launches
     def forward(self):
         """sinos_out[i] = A_i images_in[i] for every scan, one launch."""
         with torch.cuda.device(self.device):
-            N.call("ctlab_forward_project_batched", ctypes.byref(self._plan), self.config["n_cta"],
-                   N.stream_of(self._ws))
+            N.call("ctlab_forward_project_batched", ctypes.byref(self._plans["fwd"]), self.config["n_cta"],
+                   N.stream_of(self._ws["fwd"]))
 
     def back(self, accumulate=False):
         """images_out[i] (+)= A_i^T sinos_in[i] for every scan: one zeroing
         launch (unless accumulating) and one persistent launch."""
         with torch.cuda.device(self.device):
-            N.call("ctlab_back_project_batched", ctypes.byref(self._plan), int(bool(accumulate)),
-                   self.config["n_cta"], N.stream_of(self._ws))
+            N.call("ctlab_back_project_batched", ctypes.byref(self._plans["adj"]), int(bool(accumulate)),
+                   self.config_adj["n_cta"], N.stream_of(self._ws["adj"]))
 
     def forward_loop(self):
         """The same forward one scan at a time (single-scan entry points)."""
-        st = N.stream_of(self._ws)
+        st = N.stream_of(self._ws["fwd"])
         with torch.cuda.device(self.device):
             for i, p in enumerate(self.projectors):
-                o = self._loop_opts[i]
+                o = self._loop_opts_f[i]
                 if self.ndim == 3:
                     N.call("ctlab_forward_project_3d_on_the_fly_ex", N.ptr(self.images_in[i]), 1, p.n_x, p.n_y,
                            p.n_z, N.ptr(p.src), N.ptr(p.dst), int(p.src.shape[0]), N.ptr(p.M_inv), N.ptr(p.b),
@@ -244,11 +282,11 @@ class ScanBatch:
 
     def back_loop(self, accumulate=False):
         """The same adjoint one scan at a time (single-scan entry points)."""
-        st = N.stream_of(self._ws)
+        st = N.stream_of(self._ws["adj"])
         acc = int(bool(accumulate))
         with torch.cuda.device(self.device):
             for i, p in enumerate(self.projectors):
-                o = self._loop_opts[i]
+                o = self._loop_opts_a[i]
                 if self.ndim == 3:
                     N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
@@ -279,8 +317,9 @@ class ScanBatch:
         return g
 
     def autotune(self, reps=3, block_threads=(128, 256), tuner=None):
-        """Pick the fastest (block_threads, tile kind) for this batch by timing
-        forward + adjoint passes; the result is cached per batch signature."""
+        """Pick the fastest (block_threads, tile kind) for this batch, for the
+        forward and for the adjoint separately, by timing passes; the result
+        is cached per batch signature."""
         return (tuner or DEFAULT_TUNER).tune(self, reps=reps, block_threads=block_threads)
 
     def signature(self):
@@ -290,8 +329,8 @@ class ScanBatch:
 
 class Autotuner:
     """Times every candidate launch shape of a batch with CUDA events (median
-    of `reps` forward + adjoint passes after one warm-up) and keeps the
-    fastest per batch signature."""
+    of `reps` passes after one warm-up), forward and adjoint separately, and
+    keeps the fastest of each per batch signature."""
 
     def __init__(self):
         self.cache = {}
@@ -301,36 +340,38 @@ class Autotuner:
         kinds = sorted({k for p in batch.projectors for k in tile_kinds(p)})
         return [(bt, k) for bt in block_threads for k in kinds]
 
-    def _time(self, batch, reps):
-        def one():
-            if batch.has_forward:
-                batch.forward()
-            if batch.has_adjoint:
-                batch.back()
-        one()
+    def _time(self, fn, device, reps):
+        fn()
         ts = []
         for _ in range(reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            one()
+            fn()
             e1.record()
-            torch.cuda.synchronize(batch.device)
+            torch.cuda.synchronize(device)
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
 
     def tune(self, batch, reps=3, block_threads=(128, 256)):
         key = batch.signature()
         if key not in self.cache:
-            results = []
+            best, trials = {}, {}
             with torch.cuda.device(batch.device):
-                for bt, kind in self.candidates(batch, block_threads):
-                    batch.configure(block_threads=bt, kind=kind)
-                    results.append((self._time(batch, reps), bt, kind))
-            results.sort()
-            self.trials[key] = results
-            self.cache[key] = {"block_threads": results[0][1], "kind": results[0][2]}
-        best = self.cache[key]
-        return batch.configure(block_threads=best["block_threads"], kind=best["kind"])
+                for d, used, fn in (("fwd", batch.has_forward, batch.forward), ("adj", batch.has_adjoint, batch.back)):
+                    if not used:
+                        continue
+                    res = []
+                    for bt, kind in self.candidates(batch, block_threads):
+                        batch.configure(block_threads=bt, kind=kind, direction=d)
+                        res.append((self._time(fn, batch.device, reps), bt, kind))
+                    res.sort()
+                    trials[d] = res
+                    best[d] = {"block_threads": res[0][1], "kind": res[0][2]}
+            self.trials[key] = trials
+            self.cache[key] = best
+        for d, cfg in self.cache[key].items():
+            batch.configure(block_threads=cfg["block_threads"], kind=cfg["kind"], direction=d)
+        return batch.config
 
 
 DEFAULT_TUNER = Autotuner()

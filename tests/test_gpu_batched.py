@@ -87,7 +87,7 @@ def _check_against_loop(batch):
 
 
 @pytest.mark.parametrize("block_threads", [128, 256])
-@pytest.mark.parametrize("kind", ["flat", "grid32", "grid64"])
+@pytest.mark.parametrize("kind", ["flat", "grid32", "grid64", "vgrid32", "vgrid64"])
 def test_batched_2d_equals_per_scan_loop(kind, block_threads):
     from ct_laboratory_b200.batched import ScanBatch
     batch = ScanBatch(uneven_2d(), block_threads=block_threads, kind=kind)
@@ -161,8 +161,11 @@ def test_autotuner_picks_a_measured_candidate():
     tuner = Autotuner()
     cfg = batch.autotune(reps=2, tuner=tuner)
     trials = tuner.trials[batch.signature()]
-    assert len(trials) == 6 and trials == sorted(trials)
-    assert (cfg["block_threads"], cfg["kind"]) == trials[0][1:]
+    assert set(trials) == {"fwd", "adj"}
+    for d in ("fwd", "adj"):  # 2 block sizes x 5 tile kinds, each direction timed on its own
+        assert len(trials[d]) == 10 and trials[d] == sorted(trials[d])
+    assert (cfg["block_threads"], cfg["kind"]) == trials["fwd"][0][1:]
+    assert (batch.config_adj["block_threads"], batch.config_adj["kind"]) == trials["adj"][0][1:]
     again = batch.autotune(tuner=tuner)  # cached: no new trials
     assert again["kind"] == cfg["kind"] and len(tuner.trials) == 1
     _fill(batch)
