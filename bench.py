@@ -252,7 +252,7 @@ def run_ours(args, world, rank, local):
         proj = ConeBeam3DProjector(*w.n, n_view=w.n_view, det_nx=w.det_nx, det_ny=w.det_ny, sid=w.sid, sdd=w.sdd,
                                    det_spacing=w.pitch, voxel_size=w.voxel, device=dev, tile_rows=args.tile_rows,
                                    voxel_rule=args.voxel_rule, walk=args.walk,
-                                   deterministic_adjoint=args.deterministic)
+                                   deterministic_adjoint=args.deterministic, block_threads=args.block_threads)
     else:
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
                                   pixel_size=w.pixel, device=dev)
@@ -321,7 +321,8 @@ def run_ours(args, world, rank, local):
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": {"workload": w.name, "n_ray": n_ray, "volume": list(w.n),
                           "views": w.n_view, "rays_per_rank": n_ray, "l2": "flushed (512 MiB write) before each step",
-                          "tile_rows": args.tile_rows, "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
+                          "tile_rows": args.tile_rows, "block_threads": args.block_threads,
+                          "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
                           "walk": ["auto", "lane", "column"][args.walk],
                           "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
                           "parallelism": f"independent scans x{world}"},
@@ -588,6 +589,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="cone256")
     ap.add_argument("--tile-rows", type=int, default=32)
+    ap.add_argument("--block-threads", type=int, default=128, help="threads per CTA of the cone-beam launches")
     ap.add_argument("--voxel-rule", type=int, default=1, help="0 = reference midpoint rule, 1 = crossing rule")
     ap.add_argument("--walk", type=int, default=0, help="0 = auto, 1 = per-lane walk, 2 = column walk")
     ap.add_argument("--deterministic", action="store_true", help="adjoint by the voxel-driven gather")

@@ -6,8 +6,9 @@
 // tail where the GPU drains.  Here the scans of a batch (uneven image sizes,
 // view counts and geometries: fan-beam views, StaticCT rings, cone-beam
 // scans) are cut into ray tiles, laid end to end, and one launch of
-// persistent CTAs (resident CTAs per SM x SMs) pulls tiles from a device work
-// counter until the batch is done.  Scans are listed heaviest first by the
+// persistent CTAs (resident CTAs per SM x SMs) works through them: every warp
+// pulls its next slice of a tile from a device work counter until the batch
+// is done.  Scans are listed heaviest first by the
 // caller (the Python planner orders them), so the long tiles start early and
 // the short ones fill the tail.
 //
@@ -79,30 +80,29 @@ __device__ __forceinline__ int find_scan(const ScanDev* __restrict__ scans, int 
 #define CTLAB_BATCH_MIN_BLOCKS 4
 #endif
 
-// One persistent CTA: take a tile, walk its rays, repeat.  MID selects the
-// midpoint voxel rule for every scan of the batch.  Thread 0 takes the next
-// tile and the whole CTA works on it, so the warp-collective steps of the
-// column walk always see full warps.
+// Persistent warps: each warp takes the next work item -- one warp's slice
+// (32 threads) of one tile -- from the device counter, walks its rays and
+// repeats, with no CTA-wide barrier: a warp never waits for its CTA's other
+// warps or for a tile hand-off.  Items are numbered tile-major (item = tile *
+// warps_per_tile + warp slot), so the warps resident at a time work on
+// neighbouring tiles.  MID selects the midpoint voxel rule for every scan of
+// the batch.  The column walk's collective steps only need the warp itself.
 template <int NDIM, bool ADJ, bool MID>
 __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
-    batched_kernel(const ScanDev* __restrict__ scans, int n_scan, unsigned total_tiles, unsigned* __restrict__ counter) {
+    batched_kernel(const ScanDev* __restrict__ scans, int n_scan, unsigned total_items, unsigned* __restrict__ counter) {
     __shared__ XYCell cells[256 / 32][kChunk];
-    __shared__ unsigned s_tile;
-    __shared__ int s_scan;
+    const int lane = threadIdx.x & 31;
     XYCell* buf = cells[threadIdx.x >> 5];
+    const unsigned warps_per_tile = blockDim.x >> 5;
 #pragma unroll 1
     for (;;) {
-        if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(counter, 1u);
-            s_tile = t;
-            s_scan = t < total_tiles ? find_scan(scans, n_scan, t) : 0;
-        }
-        __syncthreads();
-        const unsigned t = s_tile;
-        const int si = s_scan;
-        __syncthreads();  // s_tile / s_scan may be overwritten from here on
-        if (t >= total_tiles) return;
-        const ScanDev* S = scans + si;
+        unsigned item = 0;
+        if (lane == 0) item = atomicAdd(counter, 1u);
+        item = __shfl_sync(kFullMask, item, 0);
+        if (item >= total_items) return;
+        const unsigned t = item / warps_per_tile;
+        const unsigned slot = item - t * warps_per_tile;
+        const ScanDev* S = scans + find_scan(scans, n_scan, t);
         Tiling T;
         T.n_view = S->T.n_view;
         T.n_row = S->T.n_row;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
         T.tiles_r = S->T.tiles_r;
         T.tiles_c = S->T.tiles_c;
         T.n_blocks = S->T.n_blocks;
-        const int64_t r = tile_ray_at(T, t - (unsigned)S->first_tile);
+        const int64_t r = tile_ray_at(T, t - (unsigned)S->first_tile, (int)(slot * 32 + lane));
         const float* in = ADJ ? S->sino_in : S->image_in;
         float* out = ADJ ? S->image_out : S->sino_out;
         const int64_t n_ray = S->n_ray, nvox = S->nvox;
@@ -136,6 +136,7 @@ __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
             const Affine2 A = load_affine2(S->M_inv, S->b);
             if (r >= 0) lane_ray<2, ADJ, MID>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
         }
+        __syncwarp();
     }
 }
 
@@ -271,7 +272,7 @@ static int launch_batched(const ctlab_batch* plan, bool adj, int accumulate, int
         if (rc) return rc;
     }
     CTLAB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
-    const unsigned total = (unsigned)plan->total_tiles;
+    const unsigned total = (unsigned)(plan->total_tiles * (plan->block_threads / 32));
     const int n_scan = plan->n_scan;
     void* args[] = {(void*)&table, (void*)&n_scan, (void*)&total, (void*)&counter};
     CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)plan->block_threads), args, 0, s));
@@ -314,7 +315,8 @@ extern "C" int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t
         if (rc) return rc;
         table[i].first_tile = tiles;
         tiles += table[i].T.n_blocks;
-        CTLAB_REQUIRE(tiles < kMaxBatchTiles, "batch_plan: more than 2^31 tiles in one batch");
+        CTLAB_REQUIRE(tiles * (block_threads / 32) < kMaxBatchTiles,
+                      "batch_plan: more than 2^31 warp work items in one batch");
         fwd = fwd || scans[i].image_in != nullptr;
         adj = adj || scans[i].image_out != nullptr;
     }
@@ -436,7 +438,8 @@ extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_
         CTLAB_REQUIRE(bound, "%s: scan %d binds no %s buffers", what, i, adjoint ? "adjoint" : "forward");
         table[i].first_tile = tiles;
         tiles += table[i].T.n_blocks;
-        CTLAB_REQUIRE(tiles < kMaxBatchTiles, "%s: more than 2^31 tiles in one batch", what);
+        CTLAB_REQUIRE(tiles * (block_threads / 32) < kMaxBatchTiles, "%s: more than 2^31 warp work items in one batch",
+                      what);
     }
     void* base = nullptr;
     int rc = noalloc_scratch(&base);
@@ -462,7 +465,7 @@ extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_
         rc = default_ctas(fn, block_threads, &ctas);
         if (rc) return rc;
     }
-    const unsigned total = (unsigned)tiles;
+    const unsigned total = (unsigned)(tiles * (block_threads / 32));
     int n = n_scan;
     void* args[] = {(void*)&dtable, (void*)&n, (void*)&total, (void*)&counter};
     CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)block_threads), args, 0, s));

@@ -176,20 +176,22 @@ int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& out);
 // L2-resident fraction of the volume.  A scan has at most 2^31 - 1 tiles,
 // so all tile coordinates fit 32-bit unsigned division.  `blk` is the tile
 // index (the block index of a one-scan launch).
-__device__ __forceinline__ int64_t tile_ray_at(const Tiling& T, unsigned blk) {
+// `tid` is the thread's index within the tile (threadIdx.x for one tile per
+// CTA; warp slot * 32 + lane when warps take tiles' slices on their own).
+__device__ __forceinline__ int64_t tile_ray_at(const Tiling& T, unsigned blk, int tid) {
     const unsigned per_band = (unsigned)(T.n_view * T.tiles_c);
     const unsigned tr_u = blk / per_band;
     const unsigned rem = blk - tr_u * per_band;
     const unsigned view_u = rem / (unsigned)T.tiles_c;
     const int64_t view = view_u, tr = tr_u, tc = rem - view_u * (unsigned)T.tiles_c;
-    const int lane_r = threadIdx.x % T.tile_rows;
-    const int lane_c = threadIdx.x / T.tile_rows;
+    const int lane_r = tid % T.tile_rows;
+    const int lane_c = tid / T.tile_rows;
     int64_t row = tr * T.tile_rows + lane_r;
     int64_t col = tc * T.tile_cols + lane_c;
     if (row >= T.n_row || col >= T.n_col) return -1;
     return view * T.view_stride + row * T.row_stride + col * T.col_stride;
 }
 
-__device__ __forceinline__ int64_t tile_ray(const Tiling& T) { return tile_ray_at(T, blockIdx.x); }
+__device__ __forceinline__ int64_t tile_ray(const Tiling& T) { return tile_ray_at(T, blockIdx.x, threadIdx.x); }
 
 }  // namespace ctlab

