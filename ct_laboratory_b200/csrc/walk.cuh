@@ -420,6 +420,11 @@ constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
 constexpr int kGroupFwd = 8;
 constexpr int kGroupAdj = 4;
 
+// Walk warps whose lanes all enter and leave together without per-lane clipping.
+#ifndef CTLAB_XY_UNIFORM
+#define CTLAB_XY_UNIFORM 1
+#endif
+
 struct XYCell {
     float t;  // parameter of the crossing that ends the cell
     int col;  // flat index of the cell's (i, j) column at k = 0
@@ -514,12 +519,17 @@ struct CellGroup {
     unsigned ia[NG], ib[NG];  // voxel indices, valid where the segment is positive
 };
 
-template <int NG, bool LEN>
+// UNI: every lane of the warp enters and leaves the grid at the warp's
+// t_start / t_stop (and the round's cell ends are clipped to t_stop when the
+// buffer is written), so a cell's end needs no clipping to the lane's exit
+// and t_cur only moves forward: two operations per cell fewer, the same
+// segments.
+template <int NG, bool LEN, bool UNI>
 __device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup<NG>& g, ZWalk& Z) {
 #pragma unroll
     for (int u = 0; u < NG; ++u) {
         const XYCell c = buf[q + u];
-        const float te = fminf(c.t, Z.t_end);
+        const float te = UNI ? c.t : fminf(c.t, Z.t_end);
         const float ts = fminf(Z.tnz, te);
         g.sa[u] = LEN ? __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len) : __fsub_rn(ts, Z.t_cur);
         g.ia[u] = (unsigned)(c.col + Z.kz);
@@ -530,7 +540,7 @@ __device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup<N
         }
         g.sb[u] = LEN ? __fmul_rn(__fsub_rn(te, ts), Z.len) : __fsub_rn(te, ts);
         g.ib[u] = (unsigned)(c.col + Z.kz);
-        Z.t_cur = fmaxf(Z.t_cur, te);
+        Z.t_cur = UNI ? te : fmaxf(Z.t_cur, te);
     }
 }
 
@@ -711,58 +721,77 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
     // forward: cells per step so that every step has 2 * kGroupFwd gathers in flight
     constexpr int kGF = kGroupFwd / NB > 0 ? kGroupFwd / NB : 1;
+    // Do all 32 lanes trace live rays entering and leaving at the warp's
+    // t_start / t_stop?  (Most warps of a cone-beam scan: their rays cross the
+    // volume's side faces, not its top or bottom.)
+    const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
+    auto rounds = [&](auto uni_tag) {
+        constexpr bool UNI = decltype(uni_tag)::value;
 #pragma unroll 1
-    for (int round = 0; round < max_rounds; ++round) {
-        // lane l: the l-th next x plane and the l-th next y plane (plane
-        // coordinates are exact: |p| < 2^17 in steps of 1)
-        const float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
-        const float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
-        // merged positions; on equal parameters the x crossing comes first
-        const int rx = lane + warp_rank<false>(ty, tx);
-        const int ry = lane + warp_rank<true>(tx, ty);
-        if (rx < kChunk) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
-        if (ry < kChunk) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
-        const int n_x = __popc(__ballot_sync(kFullMask, rx < kChunk));
-        __syncwarp();
-        // cells up to and including the one that ends at or after t_stop
-        const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
-        const int n_cells = min(n_in + 1, kChunk);
-        if constexpr (ADJ) {
-            // y * |v| once per lane, times each parameter span: the same
-            // segment lengths as the forward's, multiplied in another order
+        for (int round = 0; round < max_rounds; ++round) {
+            // lane l: the l-th next x plane and the l-th next y plane (plane
+            // coordinates are exact: |p| < 2^17 in steps of 1)
+            float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
+            float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
+            // merged positions; on equal parameters the x crossing comes first
+            const int rx = lane + warp_rank<false>(ty, tx);
+            const int ry = lane + warp_rank<true>(tx, ty);
+            if (UNI) {  // cell ends past the common exit are the exit
+                tx = fminf(tx, t_stop);
+                ty = fminf(ty, t_stop);
+            }
+            if (rx < kChunk) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
+            if (ry < kChunk) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
+            const int n_x = __popc(__ballot_sync(kFullMask, rx < kChunk));
+            __syncwarp();
+            // cells up to and including the one that ends at or after t_stop
+            const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
+            const int n_cells = min(n_in + 1, kChunk);
+            if constexpr (ADJ) {
+                // y * |v| once per lane, times each parameter span: the same
+                // segment lengths as the forward's, multiplied in another order
 #pragma unroll 1
-            for (int q = 0; q < n_cells; q += kGroupAdj) {
-                CellGroup<kGroupAdj> g;
-                walk_group<kGroupAdj, false>(buf, q, g, Z);
+                for (int q = 0; q < n_cells; q += kGroupAdj) {
+                    CellGroup<kGroupAdj> g;
+                    walk_group<kGroupAdj, false, UNI>(buf, q, g, Z);
 #pragma unroll
-                for (int j = 0; j < NB; ++j) {
+                    for (int j = 0; j < NB; ++j) {
 #pragma unroll
-                    for (int u = 0; u < kGroupAdj; ++u) {
-                        red_add_if(vout[j] + g.ia[u], __fmul_rn(yl[j], g.sa[u]), g.sa[u] > 0.f && j < nb);
-                        red_add_if(vout[j] + g.ib[u], __fmul_rn(yl[j], g.sb[u]), g.sb[u] > 0.f && j < nb);
+                        for (int u = 0; u < kGroupAdj; ++u) {
+                            const bool vj = NB == 1 || j < nb;  // one volume: always valid
+                            red_add_if(vout[j] + g.ia[u], __fmul_rn(yl[j], g.sa[u]), g.sa[u] > 0.f && vj);
+                            red_add_if(vout[j] + g.ib[u], __fmul_rn(yl[j], g.sb[u]), g.sb[u] > 0.f && vj);
+                        }
                     }
                 }
-            }
-        } else {
-            // the step's gathers are issued together, then accumulated in
-            // walk order, volume by volume
+            } else {
+                // the step's gathers are issued together, then accumulated in
+                // walk order, volume by volume
 #pragma unroll 1
-            for (int q = 0; q < n_cells; q += kGF) {
-                CellGroup<kGF> g;
-                walk_group<kGF, true>(buf, q, g, Z);
-                float v[NB][2 * kGF];
+                for (int q = 0; q < n_cells; q += kGF) {
+                    CellGroup<kGF> g;
+                    walk_group<kGF, true, UNI>(buf, q, g, Z);
+                    float v[NB][2 * kGF];
 #pragma unroll
-                for (int j = 0; j < NB; ++j) gather_group<kGF>(vol[j], g, v[j], pol);
+                    for (int j = 0; j < NB; ++j) gather_group<kGF>(vol[j], g, v[j], pol);
 #pragma unroll
-                for (int j = 0; j < NB; ++j) acc[j] = accumulate_group<kGF>(g, v[j], acc[j]);
+                    for (int j = 0; j < NB; ++j) acc[j] = accumulate_group<kGF>(g, v[j], acc[j]);
+                }
             }
+            if (n_in < kChunk) break;
+            __syncwarp();  // every lane is done with this round's cells
+            col += n_x * dsx + (kChunk - n_x) * dsy;
+            pnx = __fmaf_rn((float)n_x, psx, pnx);
+            pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
         }
-        if (n_in < kChunk) break;
-        __syncwarp();  // every lane is done with this round's cells
-        col += n_x * dsx + (kChunk - n_x) * dsy;
-        pnx = __fmaf_rn((float)n_x, psx, pnx);
-        pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
-    }
+    };
+#if CTLAB_XY_UNIFORM
+    if (uniform) rounds(std::true_type{});
+    else
+#else
+    (void)uniform;
+#endif
+        rounds(std::false_type{});
     if constexpr (!ADJ) {
         if (r >= 0) {
 #pragma unroll
