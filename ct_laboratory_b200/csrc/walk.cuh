@@ -417,8 +417,14 @@ constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
 // gathers of 8 cells together (up to 16 loads in flight per lane), the
 // adjoint's reductions need no results and walk 4 at a time (measured
 // fastest for each on the cone-beam benchmark scan).
-constexpr int kGroupFwd = 8;
-constexpr int kGroupAdj = 4;
+#ifndef CTLAB_XY_GROUP_FWD
+#define CTLAB_XY_GROUP_FWD 8
+#endif
+#ifndef CTLAB_XY_GROUP_ADJ
+#define CTLAB_XY_GROUP_ADJ 4
+#endif
+constexpr int kGroupFwd = CTLAB_XY_GROUP_FWD;
+constexpr int kGroupAdj = CTLAB_XY_GROUP_ADJ;
 
 // Walk warps whose lanes all enter and leave together without per-lane clipping.
 #ifndef CTLAB_XY_UNIFORM
