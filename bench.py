@@ -20,8 +20,17 @@ time is the max over ranks.  Rank 0 prints one JSON line that also holds:
                 host's cores, on a bounded sample of views (N = 1 only)
   e2e           the same metric through the public module API with pinned
                 host buffers, H2D of each step's inputs and D2H of its outputs
-                inside the timed region
+                inside the timed region (copies on a second stream, under
+                the kernels)
   clocks        nvidia-smi SM clock / throttle reasons sampled while timing
+and, at N = 1, three legs of the other workloads (each can be switched off):
+  batched       64 uneven 2-D scans: one persistent launch per direction from
+                a CUDA graph against the per-scan loop (--batched-steps 0)
+  serving       16 MAP jobs arriving at 20/s: the continuous-batching server
+                against the plain per-job estimator loop (--serve-jobs 0)
+  map           MAP on the cone scan: Lanczos k=64 preconditioner, 50
+                iterations, finite-difference gradient check, adjoint
+                identity (--map-iters 0)
 
 reference: times the reference's CPU projector (the oracle's port of its
 torch path) on the host cores, rank 0 only, K steps each a bounded sample.
