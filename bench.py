@@ -184,6 +184,7 @@ class CpuCase:
         self.w = w
         self.src = np.ascontiguousarray(src.cpu().numpy() if torch.is_tensor(src) else src)
         self.dst = np.ascontiguousarray(dst.cpu().numpy() if torch.is_tensor(dst) else dst)
+        self.M = np.asarray(M.cpu().numpy() if torch.is_tensor(M) else M, dtype=np.float64)
         self.Mi = O.minv(M.cpu().numpy() if torch.is_tensor(M) else M)
         self.b = np.ascontiguousarray(b.cpu().numpy() if torch.is_tensor(b) else b)
         if vol is None:
@@ -206,16 +207,36 @@ class CpuCase:
         return idx.size / dt, idx.size, dt
 
 
-def cpu_baseline(case, target_s=15.0):
+def cpu_baseline(case, target_s=15.0, gpu_view0=None):
+    """The oracle's port of the reference CPU path, timed; and, when the GPU
+    results for view 0 are given (forward sinogram of that view, adjoint of
+    that view's sinogram alone, and that sinogram), their errors against the
+    FP64 oracle (the reference's plane-sort Siddon in double precision) on
+    that full-size view."""
+    from oracle import oracle as O
     w = case.w
     threads = cpu_threads()
     rate, n, dt = case.rate([0], threads)  # calibration: one view
     n_views = int(max(1, min(w.n_view, math.floor(target_s * rate / case.per_view))))
     views = [int(round(i * w.n_view / n_views)) % w.n_view for i in range(n_views)]
     rate, n, dt = case.rate(views, threads)
-    return {"value": rate / 1e9, "unit": "GRays/s", "cores": threads, "kind": "port",
-            "sample": f"{n_views} of {w.n_view} views evenly spaced ({n} rays, {dt:.1f} s fwd+adj), "
-                      "extrapolated linearly (rays are independent)"}
+    out = {"value": rate / 1e9, "unit": "GRays/s", "cores": threads, "kind": "port",
+           "sample": f"{n_views} of {w.n_view} views evenly spaced ({n} rays, {dt:.1f} s fwd+adj), "
+                     "extrapolated linearly (rays are independent)"}
+    if gpu_view0 is not None and case.vol.ndim == 3:
+        f_gpu, a_gpu, y0 = (np.asarray(a, dtype=np.float64) for a in gpu_view0)
+        pv = case.per_view
+        s64, d64 = case.src[:pv].astype(np.float64), case.dst[:pv].astype(np.float64)
+        Mi64, b64 = np.linalg.inv(case.M), case.b.astype(np.float64)
+        f64 = O.fwd_planesort(case.vol, Mi64, b64, s64, d64, dtype=np.float64)
+        a64 = O.back_planesort(y0, Mi64, b64, s64, d64, case.vol.shape, dtype=np.float64)
+
+        def errs(a, ref):
+            return {"max_rel": float(np.abs(a - ref).max() / np.abs(ref).max()),
+                    "rel_l2": float(np.linalg.norm(a - ref) / np.linalg.norm(ref))}
+        out["fp64_check"] = {"rays": pv, "view": 0, "forward": errs(f_gpu, f64), "adjoint": errs(a_gpu, a64),
+                             "note": "GPU float32 (crossing rule) against the FP64 plane-sort oracle"}
+    return out
 
 
 def run_reference(args, world, rank):
@@ -323,7 +344,15 @@ def run_ours(args, world, rank, local):
         else None
     cpu = None
     if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
-        cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s)
+        view0 = None
+        if w.name.startswith("cone"):
+            pv = w.det_nx * w.det_ny
+            with torch.no_grad():
+                y0 = torch.zeros_like(y)
+                y0[:pv] = y[:pv]
+                view0 = (proj.forward_project(x)[:pv].cpu().numpy(), proj.back_project(y0).cpu().numpy(),
+                         y[:pv].cpu().numpy())
+        cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s, view0)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "GRays/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -143,3 +143,20 @@ def test_fanbeam_and_static2d_modules():
     assert rel_err(p(img).cpu().numpy(), g["fwd"]) < 1e-5
     assert rel_err(p.back_project(torch.as_tensor(g["y"]).to(DEV)).cpu().numpy(), g["back"]) < 1e-5
     assert np.array_equal(p.tvals.cpu().numpy(), g["tvals"])
+
+
+@pytest.mark.parametrize("name", ["cone3d", "affine3d", "static3d"])
+def test_autograd_gradient_matches_reference_gradient(name):
+    """d/dvol sum(y * A vol) through our autograd Function equals the
+    reference's own A^T y (its torch path, stored in the golden fixture), the
+    gradient its CTProjector3DFunction backward returns
+    (ct_projector_3d_autograd.py:160-170).  Tolerance: the spread between the
+    reference's torch and CUDA paths, 5e-5."""
+    from ct_laboratory_b200 import CTProjector3DModule
+    g = load_golden(name)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(DEV, torch.float32)  # noqa: E731
+    d = [int(v) for v in g["dims"]]
+    p = CTProjector3DModule(*d, T(g["M"]), T(g["b"]), T(g["src"]), T(g["dst"]), device=torch.device(DEV))
+    vol = T(g["vol"]).requires_grad_(True)
+    (p(vol) * T(g["y"])).sum().backward()
+    assert rel_err(vol.grad.cpu().numpy(), g["back"]) < 5e-5
