@@ -14,9 +14,10 @@ allocates once:
 (or binds caller-owned tensors given as ``buffers={"images_in": [...], ...}``).
 
 ``forward()`` computes every sinos_out[i] = A_i images_in[i] in one launch
-of persistent CTAs that pull ray tiles of all scans from a device work
-counter (libctlab_b200.so ``ctlab_forward_project_batched``); ``back()`` the
-adjoints likewise.  ``forward_loop()`` / ``back_loop()`` run the very same
+of persistent CTAs whose warps pull slices of the ray tiles of all scans
+from a device work counter (libctlab_b200.so
+``ctlab_forward_project_batched``); ``back()`` the adjoints likewise, each
+direction with its own plan and tile layout.  ``forward_loop()`` / ``back_loop()`` run the very same
 walks one scan at a time through the single-scan entry points, into the
 same buffers: the per-instance loop the batch replaces.  Forward results are
 bitwise equal between the two; adjoints up to the order of float atomics.

@@ -12,7 +12,7 @@
 //     t_out = min(t_exit,  ahead-plane parameters of the voxel)
 //     len   = (t_out - t_in) * |v|      (0 when t_out <= t_in)
 // with every plane parameter t = (p - s) * (1/v) and the per-ray set-up
-// (t_enter, t_exit, 1/v, |v|) computed exactly as siddon.cu computes them.
+// (t_enter, t_exit, 1/v, |v|) computed exactly as the walks in walk.cuh compute them.
 // These are bitwise the segment lengths the crossing-rule walk produces, so
 // the result is the exact transpose of that forward, accumulated in a fixed
 // order (panel, then row, then column): bitwise reproducible from run to run.
@@ -33,7 +33,7 @@ struct PanelDev {
     int n_u, n_v;
 };
 
-// Same set-up as lane_setup / traverse in siddon.cu.
+// Same set-up as lane_setup / traverse in walk.cuh.
 struct RaySetup {
     float s[3], inv[3], ray_len, t_enter, t_exit;
     int fixed[3];  // index along an axis the ray does not cross, else -1
