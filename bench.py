@@ -479,7 +479,10 @@ def run_batched(args, dev, flush):
             "ms_per_pass": {"graph": ms_graph, "batched": ms_eager, "per_scan_loop": ms_loop},
             "grays_s": {"graph": n_ray / ms_graph / 1e6, "batched": n_ray / ms_eager / 1e6,
                         "per_scan_loop": n_ray / ms_loop / 1e6},
-            "speedup_vs_loop": ms_loop / ms_graph, "gpu_launches_per_pass": {"graph": 3, "per_scan_loop": 128},
+            "speedup_vs_loop": ms_loop / ms_graph, "gpu_launches_per_pass": {
+                # forward; adjoint: zeroing, walk, and the add-back of the transposed scratch
+                "graph": 3 + (batch.scratch is not None),
+                "per_scan_loop": len(batch.projectors) * (2 + (batch.scratch is not None))},
             "roofline_frac": bytes_pair / (ms_graph / 1e3) / 1e9 / peak,
             "setup_s": setup_s, "autotune_s": tune_s,
             "note": "one pass = forward + adjoint of all 64 scans; L2 flushed before each pass; median of "

@@ -47,7 +47,7 @@ class Scan(ctypes.Structure):
 
     _fields_ = [("image_in", _P), ("sino_out", _P), ("sino_in", _P), ("image_out", _P), ("src", _P), ("dst", _P),
                 ("M_inv", _P), ("b", _P), ("n_ray", _I64), ("dims", _I64 * 3), ("ndim", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("opts", RayOpts)]
+                ("reserved", ctypes.c_int32), ("opts", RayOpts), ("image_scratch", _P)]
 
 
 class Batch(ctypes.Structure):
@@ -55,7 +55,7 @@ class Batch(ctypes.Structure):
 
     _fields_ = [("workspace", _P), ("total_tiles", _I64), ("n_scan", ctypes.c_int32), ("ndim", ctypes.c_int32),
                 ("block_threads", ctypes.c_int32), ("voxel_rule", ctypes.c_int32), ("has_forward", ctypes.c_int32),
-                ("has_adjoint", ctypes.c_int32), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("has_adjoint", ctypes.c_int32), ("device", ctypes.c_int32), ("has_scratch", ctypes.c_int32)]
 
 
 _SP = ctypes.POINTER(Scan)
@@ -84,6 +84,7 @@ _SIGS = {
     "ctlab_back_project_2d_on_the_fly": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _P],
     "ctlab_forward_project_2d_siddon": [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _TP, _P],
     "ctlab_back_project_2d_siddon": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P],
+    "ctlab_back_project_2d_siddon_ws": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P, _P],
     "ctlab_invert_matrix": [_P, _I, _P, _P, _P],
     "ctlab_back_project_3d_gather": [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I64, _P, _P],
     "ctlab_batch_plan": [_SP, _I32, _I32, _P, _I64, _BP, _P],

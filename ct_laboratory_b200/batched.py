@@ -77,7 +77,7 @@ def tile_kinds(p):
     grid64    2-D: 64 cells x (block_threads/64) views
     vgrid32   2-D: 32 views x (block_threads/32) cells, lanes along views (the
               same cell seen from 32 directions: the lanes' pixels are far
-              apart, so the adjoint's reductions do not collide)
+              apart)
     vgrid64   2-D: 64 views x (block_threads/64) cells
     col32     3-D detector grid: 32 detector rows x (block_threads/32) columns
               (lanes of a warp down one detector column: the column walk)
@@ -156,6 +156,9 @@ class ScanBatch:
                             raise ValueError(f"ScanBatch: buffers['{name}'] must be contiguous float32 tensors of "
                                              f"shape {tuple(s)} on {self.device}")
                 setattr(self, name, list(ts) if used else None)
+        # 2-D crossing-rule adjoint: a transposed scratch image per scan
+        self.scratch = (self._arena(shapes) if adjoint and self.ndim == 2 and self.voxel_rule == N.VOXEL_CROSSING
+                        else None)
         # heaviest rays first: long tiles start early, short ones fill the tail
         self.order = sorted(range(len(self.projectors)), key=lambda i: -_cost(self.projectors[i]))
         nbytes = N.lib.ctlab_batch_workspace_bytes(len(self.projectors))
@@ -194,6 +197,8 @@ class ScanBatch:
             s.image_in, s.sino_out = self.images_in[i].data_ptr(), self.sinos_out[i].data_ptr()
         if self.has_adjoint:
             s.sino_in, s.image_out = self.sinos_in[i].data_ptr(), self.images_out[i].data_ptr()
+            if self.scratch is not None:
+                s.image_scratch = self.scratch[i].data_ptr()
         s.src, s.dst = p.src.data_ptr(), p.dst.data_ptr()
         s.M_inv, s.b = p.M_inv.data_ptr(), p.b.data_ptr()
         s.n_ray = int(p.src.shape[0])
@@ -211,8 +216,6 @@ class ScanBatch:
             k = tile_kinds(p)
             if "col32" in k:
                 out.append("col32")
-            elif direction == "adj" and "vgrid32" in k:
-                out.append("vgrid32")
             elif "grid32" in k:
                 out.append("grid32")
             else:
@@ -222,8 +225,9 @@ class ScanBatch:
     def configure(self, block_threads=256, kind="auto", n_cta=0, direction="both"):
         """(Re)plan the batch with a tile layout: `kind` is one tile kind for
         every scan or a list with one kind per scan; "auto" takes col32 for
-        detector grids in 3-D, grid32 (forward) / vgrid32 (adjoint) for 2-D
-        view x cell grids, else flat.  `direction` ("fwd", "adj" or "both")
+        detector grids in 3-D, grid32 for 2-D view x cell grids (neighbouring
+        rays in a warp: coherent gathers, and adjoint reductions into
+        neighbouring pixels of one row), else flat.  `direction` ("fwd", "adj" or "both")
         selects the plan(s) to replace.  Returns the forward configuration
         (the adjoint's is ``config_adj``)."""
         for d in (("fwd", "adj") if direction == "both" else (direction,)):
@@ -293,9 +297,10 @@ class ScanBatch:
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
                            N.ptr(self.images_out[i]), acc, ctypes.byref(o), st)
                 else:
-                    N.call("ctlab_back_project_2d_siddon", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
+                    scratch = self.scratch[i] if self.scratch is not None else None
+                    N.call("ctlab_back_project_2d_siddon_ws", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_row, p.n_col,
-                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), st)
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), N.ptr(scratch), st)
 
     def capture(self, forward=True, adjoint=True, accumulate=False):
         """A CUDA graph of one forward and / or adjoint pass of the batch

@@ -48,6 +48,7 @@ struct ScanDev {
     Tiling T;
     int64_t first_tile;  // first tile of this scan in the batch
     int n[3], stride[3];
+    float* image_t;  // 2-D crossing-rule adjoint: transposed accumulation (or NULL)
 };
 
 struct BatchHeader {
@@ -134,21 +135,19 @@ __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
             }
         } else {
             const Affine2 A = load_affine2(S->M_inv, S->b);
-            if (r >= 0) lane_ray<2, ADJ, MID>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            if constexpr (ADJ && !MID && CTLAB_MAJOR2_WARP) {
+                major2_adjoint_warp(in, out, S->image_t, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            } else if (r >= 0) {
+                lane_ray<2, ADJ, MID>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            }
         }
         __syncwarp();
     }
 }
 
-// Zeroes every scan's image_out: blockIdx.y = scan, grid-stride in float4
-// where the buffer is 16-byte aligned.
-__global__ void batched_zero_kernel(const ScanDev* __restrict__ scans) {
-    const ScanDev* S = scans + blockIdx.y;
-    float* p = S->image_out;
-    const int64_t n = S->nvox;
-    if (p == nullptr) return;
+__device__ __forceinline__ void zero_span(float* p, int64_t n) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
         float4* q = reinterpret_cast<float4*>(p);
         const int64_t n4 = n >> 2;
@@ -156,6 +155,44 @@ __global__ void batched_zero_kernel(const ScanDev* __restrict__ scans) {
         for (int64_t i = (n4 << 2) + i0; i < n; i += stride) p[i] = 0.f;
     } else {
         for (int64_t i = i0; i < n; i += stride) p[i] = 0.f;
+    }
+}
+
+// Zeroes every scan's image_out (zero_out) and transposed scratch:
+// blockIdx.y = scan, grid-stride in float4 where the buffer is 16-byte
+// aligned.
+__global__ void batched_zero_kernel(const ScanDev* __restrict__ scans, int zero_out) {
+    const ScanDev* S = scans + blockIdx.y;
+    if (zero_out && S->image_out != nullptr) zero_span(S->image_out, S->nvox);
+    if (S->image_t != nullptr) zero_span(S->image_t, S->nvox);
+}
+
+// image_out[i0][i1] += image_t[i1][i0] for every scan with scratch
+// (blockIdx.y = scan): 32 x 32 tiles through shared memory, grid-stride over
+// the scan's tiles, so both sides are read and written coalesced.
+__global__ void __launch_bounds__(256) batched_add_transposed_kernel(const ScanDev* __restrict__ scans) {
+    __shared__ float tile[32][33];
+    const ScanDev* S = scans + blockIdx.y;
+    const float* __restrict__ T = S->image_t;
+    float* __restrict__ out = S->image_out;
+    if (T == nullptr || out == nullptr) return;
+    const int n0 = S->n[0], n1 = S->n[1];
+    const int t0 = (n0 + 31) >> 5, t1 = (n1 + 31) >> 5;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = blockIdx.x; k < t0 * t1; k += gridDim.x) {
+        const int i0b = (k / t1) << 5, i1b = (k % t1) << 5;
+        __syncthreads();  // the previous tile has been read out
+#pragma unroll
+        for (int r = ty; r < 32; r += 8) {
+            const int i1 = i1b + r, i0 = i0b + tx;
+            if (i1 < n1 && i0 < n0) tile[r][tx] = T[(int64_t)i1 * n0 + i0];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = ty; r < 32; r += 8) {
+            const int i0 = i0b + r, i1 = i1b + tx;
+            if (i0 < n0 && i1 < n1) out[(int64_t)i0 * n1 + i1] += tile[tx][r];
+        }
     }
 }
 
@@ -217,6 +254,11 @@ static int resolve_scan(const ctlab_scan& s, int64_t idx, int ndim, int block_th
         if (a < ndim) st *= s.dims[a];
     }
     if (s.n_ray == 0) D.T.n_blocks = 0;
+    // transposed accumulation: 2-D crossing-rule adjoints only
+    D.image_t = (ndim == 2 && voxel_rule == CTLAB_VOXEL_CROSSING && CTLAB_MAJOR2_WARP && s.image_out)
+                    ? s.image_scratch : nullptr;
+    CTLAB_REQUIRE(D.image_t == nullptr || (D.image_t != s.image_out && (const float*)D.image_t != s.image_in),
+                  "batch: scan %lld: image_scratch must be a buffer of its own", (long long)idx);
     return CTLAB_OK;
 }
 
@@ -258,8 +300,9 @@ static int launch_batched(const ctlab_batch* plan, bool adj, int accumulate, int
     char* ws = static_cast<char*>(plan->workspace);
     const ScanDev* table = reinterpret_cast<const ScanDev*>(ws + sizeof(BatchHeader));
     unsigned* counter = reinterpret_cast<unsigned*>(ws);
-    if (adj && !accumulate) {
-        batched_zero_kernel<<<dim3(64, (unsigned)plan->n_scan), 256, 0, s>>>(table);
+    const bool scratch = adj && plan->has_scratch;
+    if (adj && (!accumulate || scratch)) {
+        batched_zero_kernel<<<dim3(64, (unsigned)plan->n_scan), 256, 0, s>>>(table, accumulate ? 0 : 1);
         int rc = launch_status(what);
         if (rc) return rc;
     }
@@ -276,6 +319,11 @@ static int launch_batched(const ctlab_batch* plan, bool adj, int accumulate, int
     const int n_scan = plan->n_scan;
     void* args[] = {(void*)&table, (void*)&n_scan, (void*)&total, (void*)&counter};
     CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)plan->block_threads), args, 0, s));
+    if (scratch) {
+        int rc = launch_status(what);
+        if (rc) return rc;
+        batched_add_transposed_kernel<<<dim3(256, (unsigned)plan->n_scan), 256, 0, s>>>(table);
+    }
     return launch_status(what);
 }
 
@@ -309,7 +357,7 @@ extern "C" int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t
                   rule);
     std::vector<ScanDev> table((size_t)n_scan);
     int64_t tiles = 0;
-    bool fwd = false, adj = false;
+    bool fwd = false, adj = false, has_scratch = false;
     for (int32_t i = 0; i < n_scan; ++i) {
         int rc = resolve_scan(scans[i], i, ndim, block_threads, rule, table[i]);
         if (rc) return rc;
@@ -319,6 +367,7 @@ extern "C" int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t
                       "batch_plan: more than 2^31 warp work items in one batch");
         fwd = fwd || scans[i].image_in != nullptr;
         adj = adj || scans[i].image_out != nullptr;
+        has_scratch = has_scratch || table[i].image_t != nullptr;
     }
     int dev = 0;
     CTLAB_CUDA_TRY(cudaGetDevice(&dev));
@@ -338,7 +387,7 @@ extern "C" int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t
     plan->has_forward = fwd ? 1 : 0;
     plan->has_adjoint = adj ? 1 : 0;
     plan->device = dev;
-    plan->reserved = 0;
+    plan->has_scratch = has_scratch ? 1 : 0;
     return CTLAB_OK;
 }
 
@@ -383,7 +432,7 @@ namespace ctlab {
 constexpr int kNoAllocMaxScans = 64;
 constexpr size_t kNoAllocBytes = sizeof(BatchHeader) + (size_t)kNoAllocMaxScans * sizeof(ScanDev);
 
-// Every GPU that loads the library holds this array (about 12.5 KB) until
+// Every GPU that loads the library holds this array (about 13 KB) until
 // the process exits.  Calls share it: it keeps the last call's table and
 // counter, so each call rewrites the table and clears the counter.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -431,9 +480,11 @@ extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_
                   rule);
     ScanDev table[kNoAllocMaxScans];  // host stack, copied into the scratch below
     int64_t tiles = 0;
+    bool has_scratch = false;
     for (int32_t i = 0; i < n_scan; ++i) {
         int rc = resolve_scan(scans[i], i, ndim, block_threads, rule, table[i]);
         if (rc) return rc;
+        has_scratch = has_scratch || (adjoint && table[i].image_t != nullptr);
         const bool bound = adjoint ? scans[i].image_out != nullptr : scans[i].image_in != nullptr;
         CTLAB_REQUIRE(bound, "%s: scan %d binds no %s buffers", what, i, adjoint ? "adjoint" : "forward");
         table[i].first_tile = tiles;
@@ -453,8 +504,8 @@ extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_
     CTLAB_CUDA_TRY(cudaMemcpyAsync(ws + sizeof(BatchHeader), table, sizeof(ScanDev) * (size_t)n_scan,
                                    cudaMemcpyHostToDevice, s));
     CTLAB_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
-    if (adjoint && !accumulate) {
-        batched_zero_kernel<<<dim3(64, (unsigned)n_scan), 256, 0, s>>>(dtable);
+    if (adjoint && (!accumulate || has_scratch)) {
+        batched_zero_kernel<<<dim3(64, (unsigned)n_scan), 256, 0, s>>>(dtable, accumulate ? 0 : 1);
         rc = launch_status(what);
         if (rc) return rc;
     }
@@ -469,5 +520,10 @@ extern "C" int ctlab_project_batched_noalloc(const ctlab_scan* scans, int32_t n_
     int n = n_scan;
     void* args[] = {(void*)&dtable, (void*)&n, (void*)&total, (void*)&counter};
     CTLAB_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)ctas), dim3((unsigned)block_threads), args, 0, s));
+    if (has_scratch) {
+        rc = launch_status(what);
+        if (rc) return rc;
+        batched_add_transposed_kernel<<<dim3(256, (unsigned)n_scan), 256, 0, s>>>(dtable);
+    }
     return launch_status(what);
 }

@@ -10,8 +10,13 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
                                                      const float* __restrict__ src, const float* __restrict__ dst,
                                                      int64_t n_ray, const float* __restrict__ M_inv,
                                                      const float* __restrict__ bvec, GridDims<NDIM> G,
-                                                     int64_t nvox, Tiling T) {
+                                                     int64_t nvox, Tiling T, float* __restrict__ outT) {
     const int64_t r = tile_ray(T);
+    if constexpr (NDIM == 2 && ADJ && !MID && CTLAB_MAJOR2_WARP) {
+        // warp-cooperative: every lane takes part, with or without a ray
+        major2_adjoint_warp(in, out, outT, src, dst, n_ray, load_affine2(M_inv, bvec), G, nvox, r, blockIdx.y);
+        return;
+    }
     if (r < 0) return;
     AffineT<NDIM> aff;
     if constexpr (NDIM == 3) {
@@ -20,6 +25,34 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
         aff = load_affine2(M_inv, bvec);
     }
     lane_ray<NDIM, ADJ, MID>(in, out, src, dst, n_ray, aff, G, nvox, r, blockIdx.y);
+}
+
+// out[b][i0][i1] += T[b][i1][i0] for a batch of n0 x n1 images (row-major)
+// and their transposes T: 32 x 32 tiles through shared memory, so that both
+// the reads of T and the read-modify-writes of out are coalesced.  Tiles are
+// taken grid-stride: blockIdx.x strides over the tiles of image b =
+// blockIdx.y.
+__global__ void __launch_bounds__(256) add_transposed_kernel(float* __restrict__ out, const float* __restrict__ T,
+                                                             int n0, int n1, int64_t nvox) {
+    __shared__ float tile[32][33];
+    const int64_t b = blockIdx.y;
+    const int t0 = (n0 + 31) >> 5, t1 = (n1 + 31) >> 5;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = blockIdx.x; k < t0 * t1; k += gridDim.x) {
+        const int i0b = (k / t1) << 5, i1b = (k % t1) << 5;
+        __syncthreads();  // the previous tile has been read out
+#pragma unroll
+        for (int r = ty; r < 32; r += 8) {
+            const int i1 = i1b + r, i0 = i0b + tx;
+            if (i1 < n1 && i0 < n0) tile[r][tx] = T[b * nvox + (int64_t)i1 * n0 + i0];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = ty; r < 32; r += 8) {
+            const int i0 = i0b + r, i1 = i1b + tx;
+            if (i0 < n0 && i1 < n1) out[b * nvox + (int64_t)i0 * n1 + i1] += tile[tx][r];
+        }
+    }
 }
 
 // Resident CTAs per SM the register allocation of the column walk targets.
@@ -49,7 +82,7 @@ __global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
 template <int NDIM, bool ADJ>
 static int launch_siddon(const char* what, const float* in, float* out, int64_t batch, const int64_t* dims,
                          const float* src, const float* dst, int64_t n_ray, const float* M_inv, const float* b,
-                         int accumulate, const ctlab_ray_opts* tiling, void* stream) {
+                         int accumulate, const ctlab_ray_opts* tiling, void* stream, float* scratch = nullptr) {
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535], got %lld", what, (long long)batch);
     CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
     GridDims<NDIM> G;
@@ -105,10 +138,22 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
             return launch_status(what);
         }
     }
+    // 2-D crossing-rule adjoint with scratch: rays whose major axis is the
+    // image's column axis scatter into the transpose held in `scratch`,
+    // which is then added back (major2_adjoint_warp).
+    float* outT = (NDIM == 2 && ADJ && !mid && CTLAB_MAJOR2_WARP) ? scratch : nullptr;
+    if (outT) CTLAB_CUDA_TRY(cudaMemsetAsync(outT, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (mid)
-        siddon_kernel<NDIM, ADJ, true><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+        siddon_kernel<NDIM, ADJ, true><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, outT);
     else
-        siddon_kernel<NDIM, ADJ, false><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T);
+        siddon_kernel<NDIM, ADJ, false><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, outT);
+    if (outT) {
+        int rc = launch_status(what);
+        if (rc) return rc;
+        const int tiles = ((G.n[0] + 31) / 32) * ((G.n[1] + 31) / 32);
+        add_transposed_kernel<<<dim3((unsigned)(tiles < 1024 ? tiles : 1024), (unsigned)batch), 256, 0, s>>>(
+            out, outT, G.n[0], G.n[1], nvox);
+    }
     return launch_status(what);
 }
 
@@ -168,4 +213,15 @@ extern "C" int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, in
     const int64_t dims[2] = {n_row, n_col};
     return launch_siddon<2, true>("back_project_2d_siddon", sino, out, batch, dims, src, dst, n_ray, M_inv, b,
                                   accumulate, tiling, stream);
+}
+
+extern "C" int ctlab_back_project_2d_siddon_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                               const float* dst, const float* M_inv, const float* b, int64_t n_row,
+                                               int64_t n_col, float* out, int accumulate,
+                                               const ctlab_ray_opts* tiling, float* scratch, void* stream) {
+    clear_error();
+    const int64_t dims[2] = {n_row, n_col};
+    CTLAB_REQUIRE(scratch == nullptr || scratch != out, "back_project_2d_siddon_ws: scratch must not be the output");
+    return launch_siddon<2, true>("back_project_2d_siddon_ws", sino, out, batch, dims, src, dst, n_ray, M_inv, b,
+                                  accumulate, tiling, stream, scratch);
 }

@@ -33,6 +33,8 @@
 
 namespace ctlab {
 
+constexpr unsigned kFullMask = 0xffffffffu;
+
 template <int NDIM>
 using AffineT = typename std::conditional<NDIM == 3, Affine3, Affine2>::type;
 
@@ -360,6 +362,306 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
     }
 }
 
+// 2-D, crossing rule: the major-axis walk.  Each step crosses one slab of
+// the ray's major axis (the axis with the larger |v|: a pixel row for a
+// steep ray) and splits it at the minor-axis plane that falls inside, if
+// any:
+//     te = min(next major plane, t_exit)     ts = min(next minor plane, te)
+//     segment A = [t_cur, ts] in the current pixel, segment B = [ts, te] in
+//     the pixel past the minor plane (empty unless a minor plane lies inside)
+// These are the segments of traverse<2, ADJ, false> in the same order (the
+// same plane parameters, ties stepping both axes), so the results are
+// bitwise equal, with fewer steps.  A slab holds at most one minor plane
+// when |v_minor| <= kMajorRatio |v_major|: with |s|, |d| <= 4096 and grid
+// sides <= 4096 every plane parameter is within 0.002 index units of exact
+// (p - s rounds by at most 2^-11, 1/v and the product by 2^-24 relative), so
+// minor planes lie at least 1/0.97 - 0.007 > 1 major slab apart.  Other rays
+// take traverse<2>.
+// Neighbouring rays of a fan (the lanes of a warp) that enter the image at
+// the same row stay on the same row step by step, so their scattered
+// additions fall into neighbouring pixels of one row.
+#ifndef CTLAB_MAJOR2_RATIO
+#define CTLAB_MAJOR2_RATIO 0.97f
+#endif
+constexpr float kMajorRatio = CTLAB_MAJOR2_RATIO;
+
+// State of one lane's major-axis walk: the major axis's next plane, the
+// minor axis's next plane, the current pixel index.
+struct Major2 {
+    float ray_len, t_cur, t_exit;
+    float sM, iM, psM, pnM, tnM;  // major axis: start, 1/v, step sign, next plane, its parameter
+    float sm, im, psm, pnm, tnm;  // minor axis (tnm = +inf when the ray crosses none)
+    int idx, dsM, dsm;            // pixel index and its steps in the buffer walked
+    int n_major, start_major;     // major-axis size; slab index at the entry
+    bool major_axis1, transposed;
+};
+
+// Set-up of the major-axis walk, the arithmetic of traverse<2>'s start.
+// Returns 0 when the ray contributes nothing, 2 when it is outside the walk's
+// bound (the caller takes traverse<2>), 1 to walk.  With `transpose_fast`,
+// a ray whose major axis is the image's stride-1 axis indexes the image's
+// transpose (column-major: minor axis at stride 1, major at n_minor), so
+// that neighbouring rays stepping through the same major slab touch
+// neighbouring addresses.
+__device__ __forceinline__ int major2_setup(Major2& W, const float* sw, const float* dw, const GridDims<2>& G,
+                                            const Affine2& A, bool transpose_fast) {
+    float vw[2];
+    vw[0] = __fsub_rn(dw[0], sw[0]);
+    vw[1] = __fsub_rn(dw[1], sw[1]);
+    W.ray_len = sqrtf(sumsq2(vw[0], vw[1]));
+    if (!(W.ray_len >= 1e-12f)) return 0;
+    float s[2], d[2];
+    world_to_index2(A, sw[0], sw[1], s[0], s[1]);
+    world_to_index2(A, dw[0], dw[1], d[0], d[1]);
+    float va[2], inv[2];
+    float t_enter = 0.f, t_exit = 1.f;
+    bool live = true;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        va[a] = __fsub_rn(d[a], s[a]);
+        live = live && isfinite(s[a]) && isfinite(va[a]);
+        inv[a] = 0.f;
+        if (fabsf(va[a]) > 1e-12f) {
+            inv[a] = __frcp_rn(va[a]);
+            const float nf = (float)G.n[a];
+            const float lo = va[a] > 0.f ? -0.5f : nf - 0.5f;
+            const float hi = va[a] > 0.f ? nf - 0.5f : -0.5f;
+            t_enter = fmaxf(t_enter, plane_t(lo, s[a], inv[a]));
+            t_exit = fminf(t_exit, plane_t(hi, s[a], inv[a]));
+        }
+    }
+    // (selects, not indexing by the major axis: the arrays stay in registers)
+    const bool M = fabsf(va[1]) > fabsf(va[0]);
+    const float aM = fabsf(M ? va[1] : va[0]), am = fabsf(M ? va[0] : va[1]);
+    const bool fits = (M ? inv[1] : inv[0]) != 0.f && am <= kMajorRatio * aM &&
+                      fmaxf(fmaxf(fabsf(s[0]), fabsf(s[1])), fmaxf(fabsf(d[0]), fabsf(d[1]))) <= 4096.f &&
+                      G.n[0] <= 4096 && G.n[1] <= 4096;
+    if (!fits) return 2;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (inv[a] == 0.f) {  // no planes of this axis: the ray keeps one index along it
+            const int i = __float2int_rn(s[a]);
+            live = live && i >= 0 && i < G.n[a];
+        }
+    }
+    live = live && (t_enter < t_exit);
+    if (!live) return 0;
+
+    W.major_axis1 = M;
+    W.transposed = transpose_fast && (M ? G.stride[1] : G.stride[0]) == 1;
+    int stride[2];
+    stride[0] = W.transposed ? 1 : G.stride[0];  // transposed: (i0, i1) at i0 + i1 * n0
+    stride[1] = W.transposed ? G.n[0] : G.stride[1];
+    // start slabs at t_enter, as in traverse
+    int idx = 0, slab[2];
+    float pn[2], tn[2], ps[2];
+    int ds[2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (inv[a] == 0.f) {
+            slab[a] = __float2int_rn(s[a]);
+            idx += slab[a] * stride[a];
+            pn[a] = 0.f;
+            ps[a] = 0.f;
+            ds[a] = 0;
+            tn[a] = __int_as_float(0x7f800000);
+            continue;
+        }
+        const float c = __fmaf_rn(t_enter, va[a], s[a]);
+        int i = __float2int_rd(c + 0.5f);
+        if (va[a] > 0.f) {
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s[a], inv[a]) <= t_enter; ++k) ++i;
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s[a], inv[a]) > t_enter; ++k) --i;
+        } else {
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i - 0.5f, s[a], inv[a]) <= t_enter; ++k) --i;
+#pragma unroll 1
+            for (int k = 0; k < 4 && plane_t((float)i + 0.5f, s[a], inv[a]) > t_enter; ++k) ++i;
+        }
+        i = min(max(i, 0), G.n[a] - 1);
+        slab[a] = i;
+        idx += i * stride[a];
+        ps[a] = va[a] > 0.f ? 1.f : -1.f;
+        ds[a] = va[a] > 0.f ? stride[a] : -stride[a];
+        pn[a] = (float)i + 0.5f * ps[a];
+        tn[a] = plane_t(pn[a], s[a], inv[a]);
+    }
+    W.sM = M ? s[1] : s[0];
+    W.iM = M ? inv[1] : inv[0];
+    W.psM = M ? ps[1] : ps[0];
+    W.pnM = M ? pn[1] : pn[0];
+    W.tnM = M ? tn[1] : tn[0];
+    W.sm = M ? s[0] : s[1];
+    W.im = M ? inv[0] : inv[1];
+    W.psm = M ? ps[0] : ps[1];
+    W.pnm = M ? pn[0] : pn[1];
+    W.tnm = M ? tn[0] : tn[1];
+    W.dsM = M ? ds[1] : ds[0];
+    W.dsm = M ? ds[0] : ds[1];
+    W.n_major = M ? G.n[1] : G.n[0];
+    W.start_major = M ? slab[1] : slab[0];
+    W.idx = idx;
+    W.t_cur = t_enter;
+    W.t_exit = t_exit;
+    return 1;
+}
+
+// One step of the adjoint walk: the rest of the current major slab, split at
+// the minor plane inside it (if any), scattered as y * length.  Returns
+// whether the walk is done.
+__device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o, float y) {
+    const float te = fminf(W.tnM, W.t_exit);
+    const float ts = fminf(W.tnm, te);
+    const float sa = __fmul_rn(__fsub_rn(ts, W.t_cur), W.ray_len);
+    red_add_if(o + (unsigned)W.idx, __fmul_rn(y, sa), sa > 0.f);
+    if (W.tnm <= te) {
+        W.idx += W.dsm;
+        W.pnm += W.psm;
+        W.tnm = plane_t(W.pnm, W.sm, W.im);
+    }
+    const float sb = __fmul_rn(__fsub_rn(te, ts), W.ray_len);
+    red_add_if(o + (unsigned)W.idx, __fmul_rn(y, sb), sb > 0.f);
+    W.t_cur = te;
+    const bool done = !(W.tnM < W.t_exit);
+    if (!done) {
+        W.idx += W.dsM;
+        W.pnM += W.psM;
+        W.tnM = plane_t(W.pnM, W.sM, W.iM);
+    }
+    return done;
+}
+
+template <bool ADJ>
+__device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, float* __restrict__ out, float y,
+                                                 const float* sw, const float* dw, const GridDims<2>& G,
+                                                 const Affine2& A) {
+    Major2 W;
+    const int kind = major2_setup(W, sw, dw, G, A, false);
+    if (kind == 0) return 0.f;
+    if (kind == 2) return traverse<2, ADJ, false>(vol, out, y, sw, dw, G, A, 0u);
+    // Every step crosses one major plane; the walk ends at the slab holding
+    // the exit, so it takes at most n_major + 1 steps.
+    const int max_it = W.n_major + 2;
+    bool done = false;
+    if constexpr (!ADJ) {
+        float acc = 0.f;
+        const uint64_t pol = l2_policy_keep();
+#pragma unroll 1
+        for (int it = 0; it < max_it && !done; it += 4) {
+            float sa[4], sb[4];
+            int ia[4], ib[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float te = fminf(W.tnM, W.t_exit);
+                const float ts = fminf(W.tnm, te);
+                sa[q] = done ? 0.f : __fmul_rn(__fsub_rn(ts, W.t_cur), W.ray_len);
+                ia[q] = W.idx;
+                if (!done && W.tnm <= te) {
+                    W.idx += W.dsm;
+                    W.pnm += W.psm;
+                    W.tnm = plane_t(W.pnm, W.sm, W.im);
+                }
+                sb[q] = done ? 0.f : __fmul_rn(__fsub_rn(te, ts), W.ray_len);
+                ib[q] = W.idx;
+                W.t_cur = te;
+                done = done || !(W.tnM < W.t_exit);
+                if (!done) {
+                    W.idx += W.dsM;
+                    W.pnM += W.psM;
+                    W.tnM = plane_t(W.pnM, W.sM, W.iM);
+                }
+            }
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (sa[q] > 0.f) v[q] = ld_keep(vol + (unsigned)ia[q], pol);
+                if (sb[q] > 0.f) v[4 + q] = ld_keep(vol + (unsigned)ib[q], pol);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (sa[q] > 0.f) acc = __fmaf_rn(v[q], sa[q], acc);
+                if (sb[q] > 0.f) acc = __fmaf_rn(v[4 + q], sb[q], acc);
+            }
+        }
+        return acc;
+    } else {
+#pragma unroll 1
+        for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step(W, out, y);
+        return 0.f;
+    }
+}
+
+// The 2-D crossing-rule adjoint of one warp's rays, row-aligned: called by
+// all 32 lanes together (r = -1: the lane has no ray).  When every walking
+// lane has the same major axis and direction, the lanes start their walks
+// staggered so that at every step they all stand in the same major slab (a
+// lane whose ray enters the image later along the walk waits for the others
+// to reach its entry slab): a fan's neighbouring rays then scatter into
+// neighbouring pixels of one image row in the same instruction, a few
+// 32-byte sectors instead of one per lane.  With outT (an image-sized buffer
+// holding the image's transpose, zeroed), rays whose major axis is the
+// image's stride-1 axis scatter there; the caller adds it back.  The
+// segments and their values are those of traverse<2, true, false>; only the
+// order of the additions differs.
+__device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in, float* __restrict__ out,
+                                                    float* __restrict__ outT, const float* __restrict__ src,
+                                                    const float* __restrict__ dst, int64_t n_ray,
+                                                    const Affine2& A, const GridDims<2>& G, int64_t nvox,
+                                                    int64_t r, int64_t bi) {
+    float sw[2] = {0.f, 0.f}, dw[2] = {0.f, 0.f}, y = 0.f;
+    if (r >= 0) {
+        y = ld_stream(in + bi * n_ray + r);
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            sw[a] = ld_stream(src + r * 2 + a);
+            dw[a] = ld_stream(dst + r * 2 + a);
+        }
+    }
+    Major2 W;
+    const int kind = (r >= 0 && y != 0.f) ? major2_setup(W, sw, dw, G, A, outT != nullptr) : 0;
+    const bool walk = kind == 1;
+    // walking lanes with one major axis and direction: align them by slab
+    const int key = walk ? (W.major_axis1 ? 2 : 0) + (W.psM > 0.f ? 1 : 0) : -1;
+    const unsigned walkers = __ballot_sync(kFullMask, walk);
+    int delay = 0;
+    if (walkers != 0u) {
+        const int key0 = __shfl_sync(kFullMask, key, __ffs(walkers) - 1);
+        if (__all_sync(kFullMask, !walk || key == key0)) {
+            // position of the entry slab along the walk direction
+            int pos = walk ? (W.psM > 0.f ? W.start_major : -W.start_major) : 0x7fffffff;
+            int lo = pos;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lo = min(lo, __shfl_xor_sync(kFullMask, lo, o));
+            delay = walk ? pos - lo : 0;
+        }
+    }
+    float* o = walk && W.transposed ? outT : out;
+    o += bi * nvox;
+    bool done = !walk;
+    // every step crosses one major plane: at most n_major + 1 steps per lane
+    const int last = walk ? delay + W.n_major + 1 : 0;
+    // (a walk ends by itself before `last`; the bound only guards the loop)
+#pragma unroll 1
+    for (int it = 0;; ++it) {
+        if (!done && it >= delay) done = major2_adj_step(W, o, y) || it >= last;
+        if (__all_sync(kFullMask, done)) break;
+    }
+    if (kind == 2) traverse<2, true, false>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
+}
+
+// 2-D crossing-rule rays walk by major-axis slabs (traverse_major2):
+// 0 = never, 1 = adjoint only, 2 = forward and adjoint.
+#ifndef CTLAB_MAJOR2
+#define CTLAB_MAJOR2 1
+#endif
+// The 2-D crossing-rule adjoint kernels take the row-aligned warp walk
+// (major2_adjoint_warp).
+#ifndef CTLAB_MAJOR2_WARP
+#define CTLAB_MAJOR2_WARP 1
+#endif
+
 // Per-thread body of the per-lane walk: ray r (>= 0) of batch item bi.
 template <int NDIM, bool ADJ, bool MID>
 __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __restrict__ out,
@@ -375,10 +677,17 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
     if constexpr (ADJ) {
         const float y = ld_stream(in + bi * n_ray + r);
         if (y == 0.f) return;  // contributes exactly nothing
-        traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
+        if constexpr (NDIM == 2 && !MID && CTLAB_MAJOR2 >= 1)
+            traverse_major2<true>(nullptr, out + bi * nvox, y, sw, dw, G, aff);
+        else
+            traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
     } else {
-        st_stream(out + bi * n_ray + r,
-                  traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox));
+        float v;
+        if constexpr (NDIM == 2 && !MID && CTLAB_MAJOR2 >= 2)
+            v = traverse_major2<false>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff);
+        else
+            v = traverse<NDIM, false, MID>(in + bi * nvox, nullptr, 0.f, sw, dw, G, aff, (unsigned)nvox);
+        st_stream(out + bi * n_ray + r, v);
     }
 }
 
@@ -411,7 +720,6 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
 // host), so |p - s| < 2^18 and float rounding of a plane parameter (< 2^-6 of
 // a spacing) cannot close the 25 % margin.  Other warps run the per-lane walk.
 // ----------------------------------------------------------------------------
-constexpr unsigned kFullMask = 0xffffffffu;
 constexpr int kChunk = 32;  // x-y crossings produced per round, one per lane
 // Cells walked per inner step (both divide kChunk): the forward issues the
 // gathers of 8 cells together (up to 16 loads in flight per lane), the

@@ -266,6 +266,20 @@ int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray
                                  int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
                                  void* stream);
 
+/* ctlab_back_project_2d_siddon with scratch: `scratch` is NULL or device
+ * memory of batch * n_row * n_col floats (not `out`; its contents are
+ * overwritten).  Under the crossing rule, rays whose larger index-space
+ * direction component is along the image's columns (its stride-1 axis)
+ * accumulate into the images' transposes there, which are then added into
+ * `out`: neighbouring rays then add into neighbouring addresses, and the
+ * L2 performs several times fewer reduction operations.  Same segments and
+ * result, up to the order of the float additions.  No counterpart in the
+ * reference. */
+int ctlab_back_project_2d_siddon_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                    const float* dst, const float* M_inv, const float* b, int64_t n_row,
+                                    int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
+                                    float* scratch, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* Many scans in one launch                                                */
 /* ---------------------------------------------------------------------- */
@@ -297,6 +311,11 @@ typedef struct ctlab_scan {
     int32_t ndim;    /* 2 or 3 */
     int32_t reserved;
     ctlab_ray_opts opts;
+    /* NULL or dims[0] * dims[1] floats of device memory for a 2-D
+     * crossing-rule adjoint: the transposed accumulation of
+     * ctlab_back_project_2d_siddon_ws (contents overwritten).  Ignored in
+     * 3-D and under the midpoint rule. */
+    float* image_scratch;
 } ctlab_scan;
 
 /* A plan: filled by ctlab_batch_plan, owned by the caller, read by the
@@ -307,7 +326,8 @@ typedef struct ctlab_batch {
     int64_t total_tiles;
     int32_t n_scan, ndim, block_threads, voxel_rule;
     int32_t has_forward, has_adjoint;
-    int32_t device, reserved;
+    int32_t device;
+    int32_t has_scratch; /* some scan's adjoint accumulates in image_scratch */
 } ctlab_batch;
 
 /* Bytes of device workspace a plan of n_scan scans needs (-1 if n_scan is
@@ -339,8 +359,9 @@ int ctlab_batch_plan(const ctlab_scan* scans, int32_t n_scan, int32_t block_thre
 int ctlab_forward_project_batched(const ctlab_batch* plan, int32_t n_cta, void* stream);
 
 /* image_out = A^T sino_in for every scan of the plan (accumulate = 0 zeroes
- * each image_out first, 1 adds into it); one zeroing launch (if any) and one
- * persistent launch. */
+ * each image_out first, 1 adds into it); one zeroing launch (if any: image
+ * outputs, scratch buffers), one persistent launch and, when scans have
+ * image_scratch, one launch that adds the transposed parts back. */
 int ctlab_back_project_batched(const ctlab_batch* plan, int accumulate, int32_t n_cta, void* stream);
 
 /* Resident CTAs per SM x SMs of the current device for the batched kernel
@@ -359,7 +380,7 @@ int ctlab_batch_default_ctas(int32_t ndim, int adjoint, int voxel_rule, int32_t 
  * still owns every input and output buffer; the scratch those calls keep in
  * a workspace (work counter, resolved scan table) lives instead in a fixed
  * array inside the library's device image, of at most 64 scans (about
- * 12.5 KB, held on every GPU that loads the library until the process
+ * 13 KB, held on every GPU that loads the library until the process
  * exits).  More than 64 scans is rejected with CTLAB_EINVAL.  No cudaMalloc,
  * cudaFree or other allocating call is made.
  *
