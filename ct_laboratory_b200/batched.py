@@ -156,9 +156,8 @@ class ScanBatch:
                             raise ValueError(f"ScanBatch: buffers['{name}'] must be contiguous float32 tensors of "
                                              f"shape {tuple(s)} on {self.device}")
                 setattr(self, name, list(ts) if used else None)
-        # 2-D crossing-rule adjoint: a transposed scratch image per scan
-        self.scratch = (self._arena(shapes) if adjoint and self.ndim == 2 and self.voxel_rule == N.VOXEL_CROSSING
-                        else None)
+        # 2-D adjoint: a transposed scratch image per scan
+        self.scratch = self._arena(shapes) if adjoint and self.ndim == 2 else None
         # heaviest rays first: long tiles start early, short ones fill the tail
         self.order = sorted(range(len(self.projectors)), key=lambda i: -_cost(self.projectors[i]))
         nbytes = N.lib.ctlab_batch_workspace_bytes(len(self.projectors))

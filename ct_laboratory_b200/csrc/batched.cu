@@ -135,8 +135,8 @@ __global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
             }
         } else {
             const Affine2 A = load_affine2(S->M_inv, S->b);
-            if constexpr (ADJ && !MID && CTLAB_MAJOR2_WARP) {
-                major2_adjoint_warp(in, out, S->image_t, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            if constexpr (ADJ && CTLAB_MAJOR2_WARP) {
+                major2_adjoint_warp<MID>(in, out, S->image_t, S->src, S->dst, n_ray, A, G, nvox, r, 0);
             } else if (r >= 0) {
                 lane_ray<2, ADJ, MID>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
             }
@@ -254,9 +254,8 @@ static int resolve_scan(const ctlab_scan& s, int64_t idx, int ndim, int block_th
         if (a < ndim) st *= s.dims[a];
     }
     if (s.n_ray == 0) D.T.n_blocks = 0;
-    // transposed accumulation: 2-D crossing-rule adjoints only
-    D.image_t = (ndim == 2 && voxel_rule == CTLAB_VOXEL_CROSSING && CTLAB_MAJOR2_WARP && s.image_out)
-                    ? s.image_scratch : nullptr;
+    // transposed accumulation: 2-D adjoints only
+    D.image_t = (ndim == 2 && CTLAB_MAJOR2_WARP && s.image_out) ? s.image_scratch : nullptr;
     CTLAB_REQUIRE(D.image_t == nullptr || (D.image_t != s.image_out && (const float*)D.image_t != s.image_in),
                   "batch: scan %lld: image_scratch must be a buffer of its own", (long long)idx);
     return CTLAB_OK;

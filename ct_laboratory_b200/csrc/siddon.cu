@@ -12,9 +12,10 @@ __global__ void __launch_bounds__(256) siddon_kernel(const float* __restrict__ i
                                                      const float* __restrict__ bvec, GridDims<NDIM> G,
                                                      int64_t nvox, Tiling T, float* __restrict__ outT) {
     const int64_t r = tile_ray(T);
-    if constexpr (NDIM == 2 && ADJ && !MID && CTLAB_MAJOR2_WARP) {
+    if constexpr (NDIM == 2 && ADJ && CTLAB_MAJOR2_WARP) {
         // warp-cooperative: every lane takes part, with or without a ray
-        major2_adjoint_warp(in, out, outT, src, dst, n_ray, load_affine2(M_inv, bvec), G, nvox, r, blockIdx.y);
+        major2_adjoint_warp<MID>(in, out, outT, src, dst, n_ray, load_affine2(M_inv, bvec), G, nvox, r,
+                                 blockIdx.y);
         return;
     }
     if (r < 0) return;
@@ -138,10 +139,10 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
             return launch_status(what);
         }
     }
-    // 2-D crossing-rule adjoint with scratch: rays whose major axis is the
-    // image's column axis scatter into the transpose held in `scratch`,
-    // which is then added back (major2_adjoint_warp).
-    float* outT = (NDIM == 2 && ADJ && !mid && CTLAB_MAJOR2_WARP) ? scratch : nullptr;
+    // 2-D adjoint with scratch: rays whose major axis is the image's column
+    // axis scatter into the transpose held in `scratch`, which is then added
+    // back (major2_adjoint_warp).
+    float* outT = (NDIM == 2 && ADJ && CTLAB_MAJOR2_WARP) ? scratch : nullptr;
     if (outT) CTLAB_CUDA_TRY(cudaMemsetAsync(outT, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (mid)
         siddon_kernel<NDIM, ADJ, true><<<grid, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, outT);

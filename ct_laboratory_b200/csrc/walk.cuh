@@ -394,6 +394,7 @@ struct Major2 {
     int idx, dsM, dsm;            // pixel index and its steps in the buffer walked
     int n_major, start_major;     // major-axis size; slab index at the entry
     bool major_axis1, transposed;
+    float sw[2], vw[2];           // world start and direction (midpoint rule)
 };
 
 // Set-up of the major-axis walk, the arithmetic of traverse<2>'s start.
@@ -405,9 +406,11 @@ struct Major2 {
 // neighbouring addresses.
 __device__ __forceinline__ int major2_setup(Major2& W, const float* sw, const float* dw, const GridDims<2>& G,
                                             const Affine2& A, bool transpose_fast) {
-    float vw[2];
+    float* vw = W.vw;
     vw[0] = __fsub_rn(dw[0], sw[0]);
     vw[1] = __fsub_rn(dw[1], sw[1]);
+    W.sw[0] = sw[0];
+    W.sw[1] = sw[1];
     W.ray_len = sqrtf(sumsq2(vw[0], vw[1]));
     if (!(W.ray_len >= 1e-12f)) return 0;
     float s[2], d[2];
@@ -509,20 +512,35 @@ __device__ __forceinline__ int major2_setup(Major2& W, const float* sw, const fl
 }
 
 // One step of the adjoint walk: the rest of the current major slab, split at
-// the minor plane inside it (if any), scattered as y * length.  Returns
-// whether the walk is done.
-__device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o, float y) {
+// the minor plane inside it (if any), scattered as y * length.  MID: each
+// segment's voxel is the reference's rounded world midpoint, indexed with
+// Gt's strides (the buffer walked).  Returns whether the walk is done.
+template <bool MID>
+__device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o, float y, const Affine2& A,
+                                                const GridDims<2>& Gt) {
     const float te = fminf(W.tnM, W.t_exit);
     const float ts = fminf(W.tnm, te);
     const float sa = __fmul_rn(__fsub_rn(ts, W.t_cur), W.ray_len);
-    red_add_if(o + (unsigned)W.idx, __fmul_rn(y, sa), sa > 0.f);
+    int va = W.idx;
+    bool pa = sa > 0.f;
+    if constexpr (MID) {
+        va = midpoint_voxel<2>(A, W.sw, W.vw, W.t_cur, ts, Gt);
+        pa = pa && va >= 0;
+    }
+    red_add_if(o + (unsigned)va, __fmul_rn(y, sa), pa);
     if (W.tnm <= te) {
         W.idx += W.dsm;
         W.pnm += W.psm;
         W.tnm = plane_t(W.pnm, W.sm, W.im);
     }
     const float sb = __fmul_rn(__fsub_rn(te, ts), W.ray_len);
-    red_add_if(o + (unsigned)W.idx, __fmul_rn(y, sb), sb > 0.f);
+    int vb = W.idx;
+    bool pb = sb > 0.f;
+    if constexpr (MID) {
+        vb = midpoint_voxel<2>(A, W.sw, W.vw, ts, te, Gt);
+        pb = pb && vb >= 0;
+    }
+    red_add_if(o + (unsigned)vb, __fmul_rn(y, sb), pb);
     W.t_cur = te;
     const bool done = !(W.tnM < W.t_exit);
     if (!done) {
@@ -531,6 +549,33 @@ __device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o
         W.tnM = plane_t(W.pnM, W.sM, W.iM);
     }
     return done;
+}
+
+// Midpoint rule: the segments the reference forms just outside the grid
+// (edge_segments) next to the entry (DIR = -1, from the walk's start state)
+// or the exit (DIR = +1, from its end state), scattered into o with Gt's
+// strides.
+template <int DIR>
+__device__ __forceinline__ void major2_edge_adj(const Major2& W, float* __restrict__ o, float y, const Affine2& A,
+                                                const GridDims<2>& Gt) {
+    const bool M = W.major_axis1;
+    float s[2], inv[2], ps[2], p0[2];
+    s[0] = M ? W.sm : W.sM;
+    s[1] = M ? W.sM : W.sm;
+    inv[0] = M ? W.im : W.iM;
+    inv[1] = M ? W.iM : W.im;
+    ps[0] = M ? W.psm : W.psM;
+    ps[1] = M ? W.psM : W.psm;
+    // entry: the planes behind the start slabs; exit: the next planes ahead
+    const float pM = DIR < 0 ? W.pnM - W.psM : W.pnM, pm = DIR < 0 ? W.pnm - W.psm : W.pnm;
+    p0[0] = M ? pm : pM;
+    p0[1] = M ? pM : pm;
+    float el[kEdge];
+    int ev[kEdge];
+    const int ne = edge_segments<2, DIR>(A, W.sw, W.vw, s, inv, ps, p0, DIR < 0 ? W.t_cur : W.t_exit, W.ray_len,
+                                         Gt, ev, el);
+#pragma unroll
+    for (int k = 0; k < kEdge; ++k) red_add_if(o + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
 }
 
 template <bool ADJ>
@@ -588,23 +633,25 @@ __device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, 
         return acc;
     } else {
 #pragma unroll 1
-        for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step(W, out, y);
+        for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step<false>(W, out, y, A, G);
         return 0.f;
     }
 }
 
-// The 2-D crossing-rule adjoint of one warp's rays, row-aligned: called by
-// all 32 lanes together (r = -1: the lane has no ray).  When every walking
-// lane has the same major axis and direction, the lanes start their walks
-// staggered so that at every step they all stand in the same major slab (a
-// lane whose ray enters the image later along the walk waits for the others
-// to reach its entry slab): a fan's neighbouring rays then scatter into
-// neighbouring pixels of one image row in the same instruction, a few
-// 32-byte sectors instead of one per lane.  With outT (an image-sized buffer
-// holding the image's transpose, zeroed), rays whose major axis is the
-// image's stride-1 axis scatter there; the caller adds it back.  The
-// segments and their values are those of traverse<2, true, false>; only the
-// order of the additions differs.
+// The 2-D adjoint of one warp's rays, row-aligned: called by all 32 lanes
+// together (r = -1: the lane has no ray).  When every walking lane has the
+// same major axis and direction, the lanes start their walks staggered so
+// that at every step they all stand in the same major slab (a lane whose ray
+// enters the image later along the walk waits for the others to reach its
+// entry slab): a fan's neighbouring rays then scatter into neighbouring
+// pixels of one image row in the same instruction, a few 32-byte sectors
+// instead of one per lane.  With outT (an image-sized buffer holding the
+// image's transpose, zeroed), rays whose major axis is the image's stride-1
+// axis scatter there; the caller adds it back.  The segments and their
+// values are those of traverse<2, true, MID> (MID: the reference's midpoint
+// voxel rule, with its segments just outside the grid); only the order of
+// the additions differs.
+template <bool MID>
 __device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in, float* __restrict__ out,
                                                     float* __restrict__ outT, const float* __restrict__ src,
                                                     const float* __restrict__ dst, int64_t n_ray,
@@ -637,18 +684,29 @@ __device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in
             delay = walk ? pos - lo : 0;
         }
     }
-    float* o = walk && W.transposed ? outT : out;
-    o += bi * nvox;
+    const bool tr = walk && W.transposed;
+    float* o = (tr ? outT : out) + bi * nvox;
+    GridDims<2> Gt = G;  // the strides of the buffer walked
+    if (tr) {
+        Gt.stride[0] = 1;
+        Gt.stride[1] = G.n[0];
+    }
+    if constexpr (MID) {
+        if (walk) major2_edge_adj<-1>(W, o, y, A, Gt);
+    }
     bool done = !walk;
     // every step crosses one major plane: at most n_major + 1 steps per lane
-    const int last = walk ? delay + W.n_major + 1 : 0;
     // (a walk ends by itself before `last`; the bound only guards the loop)
+    const int last = walk ? delay + W.n_major + 1 : 0;
 #pragma unroll 1
     for (int it = 0;; ++it) {
-        if (!done && it >= delay) done = major2_adj_step(W, o, y) || it >= last;
+        if (!done && it >= delay) done = major2_adj_step<MID>(W, o, y, A, Gt) || it >= last;
         if (__all_sync(kFullMask, done)) break;
     }
-    if (kind == 2) traverse<2, true, false>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
+    if constexpr (MID) {
+        if (walk) major2_edge_adj<1>(W, o, y, A, Gt);
+    }
+    if (kind == 2) traverse<2, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, A, (unsigned)nvox);
 }
 
 // 2-D crossing-rule rays walk by major-axis slabs (traverse_major2):
@@ -656,7 +714,7 @@ __device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in
 #ifndef CTLAB_MAJOR2
 #define CTLAB_MAJOR2 1
 #endif
-// The 2-D crossing-rule adjoint kernels take the row-aligned warp walk
+// The 2-D adjoint kernels take the row-aligned warp walk
 // (major2_adjoint_warp).
 #ifndef CTLAB_MAJOR2_WARP
 #define CTLAB_MAJOR2_WARP 1

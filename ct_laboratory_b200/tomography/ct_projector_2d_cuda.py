@@ -73,14 +73,13 @@ def forward_project_2d_siddon(image, M_inv, b, src, dst, tiling=None):
 
 def back_project_2d_siddon(sinogram, M_inv, b, src, dst, n_row, n_col, tiling=None):
     """Exact adjoint of forward_project_2d_siddon, always batched [B, R, C].
-    Under the crossing rule the rays running along the image's columns
-    accumulate in a transposed scratch image (ctlab_back_project_2d_siddon_ws)."""
+    Rays running along the image's columns accumulate in a transposed
+    scratch image (ctlab_back_project_2d_siddon_ws)."""
     sino = sinogram.contiguous()
     _check(src, dst, M_inv, b, sino)
     batch, n_ray = (1, sino.shape[0]) if sino.dim() == 1 else sino.shape
     out = torch.empty((batch, n_row, n_col), device=sino.device, dtype=torch.float32)
-    crossing = tiling is not None and tiling.voxel_rule == N.VOXEL_CROSSING
-    scratch = torch.empty_like(out) if crossing and n_ray > 0 else None
+    scratch = torch.empty_like(out) if n_ray > 0 else None
     with torch.cuda.device(sino.device):
         N.call("ctlab_back_project_2d_siddon_ws", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst), N.ptr(M_inv),
                N.ptr(b), n_row, n_col, N.ptr(out), 0, N.tiling_ref(tiling), N.ptr(scratch), N.stream_of(sino))

@@ -268,13 +268,12 @@ int ctlab_back_project_2d_siddon(const float* sino, int64_t batch, int64_t n_ray
 
 /* ctlab_back_project_2d_siddon with scratch: `scratch` is NULL or device
  * memory of batch * n_row * n_col floats (not `out`; its contents are
- * overwritten).  Under the crossing rule, rays whose larger index-space
- * direction component is along the image's columns (its stride-1 axis)
- * accumulate into the images' transposes there, which are then added into
- * `out`: neighbouring rays then add into neighbouring addresses, and the
- * L2 performs several times fewer reduction operations.  Same segments and
- * result, up to the order of the float additions.  No counterpart in the
- * reference. */
+ * overwritten).  Rays whose larger index-space direction component is
+ * along the image's columns (its stride-1 axis) accumulate into the images'
+ * transposes there, which are then added into `out`: neighbouring rays then
+ * add into neighbouring addresses, and the L2 performs several times fewer
+ * reduction operations.  Same segments and result, either voxel rule, up to
+ * the order of the float additions.  No counterpart in the reference. */
 int ctlab_back_project_2d_siddon_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                     const float* dst, const float* M_inv, const float* b, int64_t n_row,
                                     int64_t n_col, float* out, int accumulate, const ctlab_ray_opts* tiling,
@@ -311,10 +310,9 @@ typedef struct ctlab_scan {
     int32_t ndim;    /* 2 or 3 */
     int32_t reserved;
     ctlab_ray_opts opts;
-    /* NULL or dims[0] * dims[1] floats of device memory for a 2-D
-     * crossing-rule adjoint: the transposed accumulation of
-     * ctlab_back_project_2d_siddon_ws (contents overwritten).  Ignored in
-     * 3-D and under the midpoint rule. */
+    /* NULL or dims[0] * dims[1] floats of device memory for a 2-D adjoint:
+     * the transposed accumulation of ctlab_back_project_2d_siddon_ws
+     * (contents overwritten).  Ignored in 3-D. */
     float* image_scratch;
 } ctlab_scan;
 

@@ -1,4 +1,4 @@
-"""The 2-D crossing-rule adjoint with transposed scratch
+"""The 2-D adjoint with transposed scratch
 (ctlab_back_project_2d_siddon_ws, ScanBatch's image_scratch).
 
 Rays whose larger index-space direction component runs along the image's
@@ -7,7 +7,9 @@ the end; the lanes of a warp walk row-aligned.  The segments are those of the
 per-lane crossing-rule walk, so the result equals the scratch-free adjoint up
 to the order of the float additions (tolerance 1e-5, the projector
 tolerance), and the oracle (the reference's plane-sort walk, float32, on
-the image embedded as a one-voxel-thick volume) within the same 1e-5.
+the image embedded as a one-voxel-thick volume) within the same 1e-5, under
+both voxel rules (the midpoint rule with the reference's segments just
+outside the grid).
 Images are non-square so that a mix-up of the transposed strides shows;
 views cover the full circle so that every warp kind occurs (rays along rows,
 along columns, near 45 degrees, mixed within a warp).
@@ -31,11 +33,11 @@ def _fan(n_row, n_col, n_view, n_det, pixel, seed=0):
     return [t.to(DEV).contiguous() for t in (src, dst, M, b)]
 
 
-def _crossing_opts(n_view, n_det):
+def _crossing_opts(n_view, n_det, rule=1):
     from ct_laboratory_b200 import _native as N
     # rays [view][cell], lanes of a warp along cells (neighbouring rays)
     return N.tiling(1, n_det, n_view, n_det * n_view, 1, n_det, tile_rows=32, block_threads=128,
-                    voxel_rule=N.VOXEL_CROSSING)
+                    voxel_rule=N.VOXEL_CROSSING if rule == 1 else N.VOXEL_MIDPOINT)
 
 
 def _adjoint(sino, src, dst, Mi, b, n_row, n_col, opts, scratch, out=None, accumulate=0):
@@ -60,14 +62,17 @@ def _embed_3d(src, dst, Mi, b):
     return s3, d3, M3, b3
 
 
+@pytest.mark.parametrize("rule", ["crossing", "midpoint", "midpoint-flat"])
 @pytest.mark.parametrize("shape", [(40, 56), (56, 40), (64, 64)])
-def test_scratch_adjoint_matches_plain_and_oracle(shape):
+def test_scratch_adjoint_matches_plain_and_oracle(shape, rule):
+    """Both voxel rules; the midpoint rule (the reference's) also without a
+    tiling (consecutive rays per warp), the projector modules' default."""
     from ct_laboratory_b200.tomography._common import inverse
     n_row, n_col = shape
     n_view, n_det = 45, 96
     src, dst, M, b = _fan(n_row, n_col, n_view, n_det, pixel=64.0 / max(shape))
     Mi = inverse(M)
-    opts = _crossing_opts(n_view, n_det)
+    opts = None if rule == "midpoint-flat" else _crossing_opts(n_view, n_det, 1 if rule == "crossing" else 0)
     g = torch.Generator(device=DEV).manual_seed(1)
     sino = torch.rand(3, n_view * n_det, device=DEV, generator=g)
     scratch = torch.full((3, n_row, n_col), float("nan"), device=DEV)  # contents must not matter
