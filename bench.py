@@ -471,18 +471,23 @@ def run_batched(args, dev, flush):
         ms_loop = timed(lambda: (batch.forward_loop(), batch.back_loop()))
     n_ray = sum(int(p.src.shape[0]) for p in batch.projectors)
     bytes_pair = 2 * (4 * SEGMENTS["batch64"] + 4 * n_ray)
+    # kernels per pass.  Persistent: forward 1; adjoint zeroing, walk and (2-D)
+    # the add-back of the transposed scratch.  Loop: one launch per scan and
+    # direction, plus one add-back per 2-D scan.
+    n_scan, tr = len(batch.projectors), int(batch.scratch is not None)
+    per_fwd = {"persistent": 1, "loop": n_scan}
+    per_adj = {"persistent": 2 + tr, "loop": n_scan * (1 + tr)}
+    launches_graph = per_fwd[cfg["mode"]] + per_adj[batch.config_adj["mode"]]
+    launches_loop = per_fwd["loop"] + per_adj["loop"]
     peak, _ = peaks()
     del graph
     return {"workload": "batch64", "n_scan": len(batch.projectors), "n_ray": n_ray, "segments": SEGMENTS["batch64"],
-            "tile": {"forward": {k: cfg[k] for k in ("block_threads", "kind", "n_cta")},
-                     "adjoint": {k: batch.config_adj[k] for k in ("block_threads", "kind", "n_cta")}},
+            "tile": {"forward": {k: cfg[k] for k in ("block_threads", "kind", "n_cta", "mode")},
+                     "adjoint": {k: batch.config_adj[k] for k in ("block_threads", "kind", "n_cta", "mode")}},
             "ms_per_pass": {"graph": ms_graph, "batched": ms_eager, "per_scan_loop": ms_loop},
             "grays_s": {"graph": n_ray / ms_graph / 1e6, "batched": n_ray / ms_eager / 1e6,
                         "per_scan_loop": n_ray / ms_loop / 1e6},
-            "speedup_vs_loop": ms_loop / ms_graph, "gpu_launches_per_pass": {
-                # forward; adjoint: zeroing, walk, and the add-back of the transposed scratch
-                "graph": 3 + (batch.scratch is not None),
-                "per_scan_loop": len(batch.projectors) * (2 + (batch.scratch is not None))},
+            "speedup_vs_loop": ms_loop / ms_graph, "gpu_launches_per_pass": {"graph": launches_graph, "per_scan_loop": launches_loop},
             "roofline_frac": bytes_pair / (ms_graph / 1e3) / 1e9 / peak,
             "setup_s": setup_s, "autotune_s": tune_s,
             "note": "one pass = forward + adjoint of all 64 scans; L2 flushed before each pass; median of "

@@ -22,8 +22,11 @@ walks one scan at a time through the single-scan entry points, into the
 same buffers: the per-instance loop the batch replaces.  Forward results are
 bitwise equal between the two; adjoints up to the order of float atomics.
 
-Tile shapes (rays per CTA and how they are laid over each scan's detector)
-are chosen by ``autotune()``, which times the candidates on the batch itself
+Each direction has a mode: the persistent launch, or the loop of
+single-scan launches (the default for the 3-D forward, where the
+single-scan column walk is faster on large scans).  Tile shapes (rays per
+CTA and how they are laid over each scan's detector) and the modes are
+chosen by ``autotune()``, which times the candidates on the batch itself
 and caches the winner per batch signature.  ``capture()`` records forward
 and / or adjoint into a ``torch.cuda.CUDAGraph`` for replay.
 
@@ -221,14 +224,22 @@ class ScanBatch:
                 out.append("flat")
         return out
 
-    def configure(self, block_threads=256, kind="auto", n_cta=0, direction="both"):
+    def configure(self, block_threads=256, kind="auto", n_cta=0, direction="both", mode="auto"):
         """(Re)plan the batch with a tile layout: `kind` is one tile kind for
         every scan or a list with one kind per scan; "auto" takes col32 for
         detector grids in 3-D, grid32 for 2-D view x cell grids (neighbouring
         rays in a warp: coherent gathers, and adjoint reductions into
         neighbouring pixels of one row), else flat.  `direction` ("fwd", "adj" or "both")
-        selects the plan(s) to replace.  Returns the forward configuration
-        (the adjoint's is ``config_adj``)."""
+        selects the plan(s) to replace.  `mode` is how forward() / back() run
+        that direction: "persistent" (one launch over all scans) or "loop"
+        (the single-scan kernels scan by scan, with the same tile layouts);
+        "auto" takes the loop for the 3-D forward, whose single-scan column
+        walk is faster than the persistent kernel's on scans of millions of
+        rays (8.75 against 9.98 ms on the cone256 scan), and the persistent
+        launch otherwise.  Returns the forward configuration (the adjoint's
+        is ``config_adj``)."""
+        if mode not in ("auto", "persistent", "loop"):
+            raise ValueError(f"ScanBatch: mode must be 'auto', 'persistent' or 'loop' (got {mode!r})")
         for d in (("fwd", "adj") if direction == "both" else (direction,)):
             k = self._default_kinds(d) if kind == "auto" else kind
             arr = (N.Scan * len(self.projectors))(*[self._scan(i, k, block_threads) for i in self.order])
@@ -242,7 +253,8 @@ class ScanBatch:
                     N.call("ctlab_batch_default_ctas", self.ndim, int(d == "adj"), self.voxel_rule,
                            int(block_threads), ctypes.byref(v))
                     ctas = v.value
-            cfg = {"block_threads": int(block_threads), "kind": k, "n_cta": int(ctas)}
+            m = mode if mode != "auto" else ("loop" if d == "fwd" and self.ndim == 3 else "persistent")
+            cfg = {"block_threads": int(block_threads), "kind": k, "n_cta": int(ctas), "mode": m}
             opts = [_opts(self.projectors[i], k if isinstance(k, str) else k[i], self.voxel_rule, block_threads)
                     for i in range(len(self.projectors))]
             if d == "fwd":
@@ -257,14 +269,21 @@ class ScanBatch:
 
     # ------------------------------------------------------------ launches
     def forward(self):
-        """sinos_out[i] = A_i images_in[i] for every scan, one launch."""
+        """sinos_out[i] = A_i images_in[i] for every scan: one launch, or the
+        per-scan loop when the forward's mode is "loop"."""
+        if self.config["mode"] == "loop":
+            return self.forward_loop()
         with torch.cuda.device(self.device):
             N.call("ctlab_forward_project_batched", ctypes.byref(self._plans["fwd"]), self.config["n_cta"],
                    N.stream_of(self._ws["fwd"]))
 
     def back(self, accumulate=False):
         """images_out[i] (+)= A_i^T sinos_in[i] for every scan: one zeroing
-        launch (unless accumulating) and one persistent launch."""
+        launch (unless accumulating) and one persistent launch (and for 2-D
+        scans the add-back of the transposed scratch), or the per-scan loop
+        when the adjoint's mode is "loop"."""
+        if self.config_adj["mode"] == "loop":
+            return self.back_loop(accumulate)
         with torch.cuda.device(self.device):
             N.call("ctlab_back_project_batched", ctypes.byref(self._plans["adj"]), int(bool(accumulate)),
                    self.config_adj["n_cta"], N.stream_of(self._ws["adj"]))
@@ -343,7 +362,7 @@ class Autotuner:
 
     def candidates(self, batch, block_threads):
         kinds = sorted({k for p in batch.projectors for k in tile_kinds(p)})
-        return [(bt, k) for bt in block_threads for k in kinds]
+        return [(bt, k, m) for m in ("persistent", "loop") for bt in block_threads for k in kinds]
 
     def _time(self, fn, device, reps):
         fn()
@@ -366,16 +385,16 @@ class Autotuner:
                     if not used:
                         continue
                     res = []
-                    for bt, kind in self.candidates(batch, block_threads):
-                        batch.configure(block_threads=bt, kind=kind, direction=d)
-                        res.append((self._time(fn, batch.device, reps), bt, kind))
+                    for bt, kind, mode in self.candidates(batch, block_threads):
+                        batch.configure(block_threads=bt, kind=kind, direction=d, mode=mode)
+                        res.append((self._time(fn, batch.device, reps), bt, kind, mode))
                     res.sort()
                     trials[d] = res
-                    best[d] = {"block_threads": res[0][1], "kind": res[0][2]}
+                    best[d] = {"block_threads": res[0][1], "kind": res[0][2], "mode": res[0][3]}
             self.trials[key] = trials
             self.cache[key] = best
         for d, cfg in self.cache[key].items():
-            batch.configure(block_threads=cfg["block_threads"], kind=cfg["kind"], direction=d)
+            batch.configure(block_threads=cfg["block_threads"], kind=cfg["kind"], direction=d, mode=cfg["mode"])
         return batch.config
 
 

@@ -77,8 +77,14 @@ __device__ __forceinline__ int find_scan(const ScanDev* __restrict__ scans, int 
 }
 
 // Resident CTAs per SM the register allocation of the batched kernels targets.
+// The 3-D forward targets 3: inside the persistent loop its column walk
+// needs more than the 64 registers a thread gets at 4 (it spilled 228 bytes
+// there and measured 9.98 ms on the cone256 scan, 9.69 ms at 3).
 #ifndef CTLAB_BATCH_MIN_BLOCKS
 #define CTLAB_BATCH_MIN_BLOCKS 4
+#endif
+#ifndef CTLAB_BATCH_MIN_BLOCKS_3D_FWD
+#define CTLAB_BATCH_MIN_BLOCKS_3D_FWD 3
 #endif
 
 // Persistent warps: each warp takes the next work item -- one warp's slice
@@ -89,7 +95,7 @@ __device__ __forceinline__ int find_scan(const ScanDev* __restrict__ scans, int 
 // neighbouring tiles.  MID selects the midpoint voxel rule for every scan of
 // the batch.  The column walk's collective steps only need the warp itself.
 template <int NDIM, bool ADJ, bool MID>
-__global__ void __launch_bounds__(256, CTLAB_BATCH_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, (NDIM == 3 && !ADJ) ? CTLAB_BATCH_MIN_BLOCKS_3D_FWD : CTLAB_BATCH_MIN_BLOCKS)
     batched_kernel(const ScanDev* __restrict__ scans, int n_scan, unsigned total_items, unsigned* __restrict__ counter) {
     __shared__ XYCell cells[256 / 32][kChunk];
     const int lane = threadIdx.x & 31;

@@ -99,7 +99,10 @@ def test_batched_2d_equals_per_scan_loop(kind, block_threads):
 def test_batched_3d_equals_per_scan_loop(kind):
     from ct_laboratory_b200.batched import ScanBatch
     batch = ScanBatch(uneven_3d(), kind=kind)
+    assert batch.config["mode"] == "loop" and batch.config_adj["mode"] == "persistent"  # the 3-D defaults
     _fill(batch)
+    _check_against_loop(batch)
+    batch.configure(kind=kind, mode="persistent")  # and the persistent forward
     _check_against_loop(batch)
 
 
@@ -162,10 +165,11 @@ def test_autotuner_picks_a_measured_candidate():
     cfg = batch.autotune(reps=2, tuner=tuner)
     trials = tuner.trials[batch.signature()]
     assert set(trials) == {"fwd", "adj"}
-    for d in ("fwd", "adj"):  # 2 block sizes x 5 tile kinds, each direction timed on its own
-        assert len(trials[d]) == 10 and trials[d] == sorted(trials[d])
-    assert (cfg["block_threads"], cfg["kind"]) == trials["fwd"][0][1:]
-    assert (batch.config_adj["block_threads"], batch.config_adj["kind"]) == trials["adj"][0][1:]
+    for d in ("fwd", "adj"):  # 2 modes x 2 block sizes x 5 tile kinds, each direction timed on its own
+        assert len(trials[d]) == 20 and trials[d] == sorted(trials[d])
+    assert (cfg["block_threads"], cfg["kind"], cfg["mode"]) == trials["fwd"][0][1:]
+    assert (batch.config_adj["block_threads"], batch.config_adj["kind"], batch.config_adj["mode"]) == \
+        trials["adj"][0][1:]
     again = batch.autotune(tuner=tuner)  # cached: no new trials
     assert again["kind"] == cfg["kind"] and len(tuner.trials) == 1
     _fill(batch)
