@@ -2,25 +2,22 @@
 // the uint16 compressor and the 2-D incremental-march kernels.
 //
 // Layout: the reference's tables are row-major [n_ray, n_int]
-// (ct_projector_3d.cu:117, :290).  Its kernels give each thread a whole row,
-// so adjacent lanes read addresses 4*n_int bytes apart.  Here a warp owns one
-// ray and its lanes own consecutive segments: every table load is a
-// contiguous 128-byte (float) or 64-byte (uint16) warp access and the row is
-// read exactly once.  Forward sums are reduced across the warp; the
-// compressed decode t_i = start + (sum_{j<=i} delta_j) * scale
-// (ct_projector_3d.cu:126-132) becomes a warp inclusive scan.
+// (ct_projector_3d.cu:117, :290), one row per ray, and its kernels give each
+// thread a whole row; the projectors here do the same (one lane per ray, the
+// row read front to back through the L1, segments added in the reference's
+// order), but skip the entries past a row's last hit at the cost of a load
+// and a compare each.  A warp that owned one ray, its lanes taking
+// consecutive segments (coalesced row loads, a warp scan for the uint16
+// decode, a warp reduction for the sum), measured slower on a 2.9 M-ray
+// StaticCT scan (14.2 / 12.4 ms against 10.0 / 10.3 ms forward / adjoint from
+// the uint16 table): its 32 lanes gather from 32 voxels strung along one ray,
+// where neighbouring lanes on neighbouring detector rows share most of their
+// x-y path.  The table builders keep a warp per ray.
 #include "common.cuh"
 
 namespace ctlab {
 
 constexpr int kWarpsPerBlock = 8;
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
 
 // Per-segment work of the reference's table kernels: world end points
 // s + t*v, world segment length, rounded midpoint voxel
@@ -60,16 +57,24 @@ struct Dims {
 };
 
 // ----------------------------------------------------------------------------
-// float tvals: forward / adjoint (one warp per ray)
+// Lane-per-ray table projectors.  Each lane walks its own row front to back,
+// as the reference's kernels do (ct_projector_3d.cu:117-160, :290-330), and
+// adds its segments in the reference's order.  The row entries past the last
+// hit cost next to nothing: a float row ends at its first +inf (rows are
+// sorted, so the rest is +inf too); a uint16 delta of 0 (an +inf entry or a
+// tie) leaves t unchanged, a zero-length segment the reference skips as well,
+// so the lane moves straight to the next entry.  Rows are read through the
+// L1 (each lane's 32-byte sector serves 8 float or 16 uint16 entries), and a
+// lane's gathers / reductions are those of one ray.
 // ----------------------------------------------------------------------------
 template <int NDIM, bool ADJ>
-__global__ void __launch_bounds__(256) tvals_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                    const float* __restrict__ tvals, int n_int,
-                                                    const float* __restrict__ src, const float* __restrict__ dst,
-                                                    int64_t n_ray, const float* __restrict__ M_inv,
-                                                    const float* __restrict__ bvec, Dims D, int64_t nvox) {
-    const int lane = threadIdx.x & 31;
-    const int64_t r = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(256) tvals_lane_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                         const float* __restrict__ tvals, int n_int,
+                                                         const float* __restrict__ src,
+                                                         const float* __restrict__ dst, int64_t n_ray,
+                                                         const float* __restrict__ M_inv,
+                                                         const float* __restrict__ bvec, Dims D, int64_t nvox) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_ray) return;
     const int64_t bi = blockIdx.y;
     Affine3 A3;
@@ -82,50 +87,43 @@ __global__ void __launch_bounds__(256) tvals_kernel(const float* __restrict__ in
         sw[a] = __ldg(src + r * NDIM + a);
         vw[a] = __fsub_rn(__ldg(dst + r * NDIM + a), sw[a]);
     }
-    const float* row = tvals + r * n_int;
     float y = 0.f;
     if constexpr (ADJ) {
         y = __ldg(in + bi * n_ray + r);
         if (y == 0.f) return;
     }
+    const float* row = tvals + r * n_int;
     const float* vol = in + bi * nvox;
     float* vout = out + bi * nvox;
     float acc = 0.f;
-    const float kInf = __int_as_float(0x7f800000);
-    for (int base = 0; base < n_int - 1; base += 32) {
-        const int i = base + lane;
-        const float t0 = i < n_int ? __ldg(row + i) : kInf;
-        float t1 = __shfl_down_sync(kFull, t0, 1);
-        if (lane == 31) t1 = (i + 1 < n_int) ? __ldg(row + i + 1) : kInf;
-        if (i < n_int - 1 && !isinf(t0) && !isinf(t1)) {
+    float t0 = __ldg(row);
+    if (!isinf(t0)) {
+#pragma unroll 1
+        for (int i = 1; i < n_int; ++i) {
+            const float t1 = __ldg(row + i);
+            if (isinf(t1)) break;
             float len;
             const int v = seg_world<NDIM>(sw, vw, t0, t1, D.n, A3, A2, len);
             if (v >= 0) {
                 if constexpr (ADJ) atomicAdd(vout + v, __fmul_rn(y, len));
                 else acc = __fmaf_rn(__ldg(vol + v), len, acc);
             }
+            t0 = t1;
         }
     }
-    if constexpr (!ADJ) {
-        acc = warp_sum(acc);
-        if (lane == 0) out[bi * n_ray + r] = acc;
-    }
+    if constexpr (!ADJ) out[bi * n_ray + r] = acc;
 }
 
-// ----------------------------------------------------------------------------
-// uint16-compressed tvals: forward / adjoint (one warp per ray)
-// ----------------------------------------------------------------------------
 template <bool ADJ>
-__global__ void __launch_bounds__(256) compressed_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                         const uint16_t* __restrict__ tq,
-                                                         const float* __restrict__ t_start,
-                                                         const float* __restrict__ t_scale, int n_int,
-                                                         const float* __restrict__ src,
-                                                         const float* __restrict__ dst, int64_t n_ray,
-                                                         const float* __restrict__ M_inv,
-                                                         const float* __restrict__ bvec, Dims D, int64_t nvox) {
-    const int lane = threadIdx.x & 31;
-    const int64_t r = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(256) compressed_lane_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                              const uint16_t* __restrict__ tq,
+                                                              const float* __restrict__ t_start,
+                                                              const float* __restrict__ t_scale, int n_int,
+                                                              const float* __restrict__ src,
+                                                              const float* __restrict__ dst, int64_t n_ray,
+                                                              const float* __restrict__ M_inv,
+                                                              const float* __restrict__ bvec, Dims D, int64_t nvox) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_ray) return;
     const int64_t bi = blockIdx.y;
     const Affine3 A = load_affine3(M_inv, bvec);
@@ -145,50 +143,36 @@ __global__ void __launch_bounds__(256) compressed_kernel(const float* __restrict
     const float* vol = in + bi * nvox;
     float* vout = out + bi * nvox;
     float acc = 0.f;
-    unsigned carry = 0;
-    for (int base = 0; base < n_int - 1; base += 32) {
-        const int i = base + lane;  // segment i spans entries i and i+1
-        const unsigned dq = (i < n_int - 1) ? (unsigned)__ldg(row + i + 1) : 0u;
-        unsigned x = dq;
+    // world point of the current segment start: t0 = start (ct_projector_3d.cu:129)
+    float p0[3];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned yv = __shfl_up_sync(kFull, x, o);
-            if (lane >= o) x += yv;
-        }
-        const unsigned k1 = carry + x;
-        const unsigned k0 = k1 - dq;
-        carry += __shfl_sync(kFull, x, 31);
-        if (i < n_int - 1) {
-            // t = start + (float)k_sum * scale, one fused multiply-add
-            // (ct_projector_3d.cu:129); the first segment starts at `start`.
-            const float t1 = __fmaf_rn(__uint2float_rn(k1), scale, start);
-            const float t0 = (i == 0) ? start : __fmaf_rn(__uint2float_rn(k0), scale, start);
-            float p0[3], p1[3];
+    for (int a = 0; a < 3; ++a) p0[a] = __fmaf_rn(start, vw[a], sw[a]);
+    unsigned k = 0;  // running sum of the deltas, in unsigned int as the reference
+#pragma unroll 1
+    for (int i = 1; i < n_int; ++i) {
+        const unsigned dq = (unsigned)__ldg(row + i);
+        if (dq == 0u) continue;  // t1 == t0: a zero-length segment
+        k += dq;
+        const float t1 = __fmaf_rn(__uint2float_rn(k), scale, start);
+        float p1[3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                p0[a] = __fmaf_rn(t0, vw[a], sw[a]);
-                p1[a] = __fmaf_rn(t1, vw[a], sw[a]);
-            }
-            const float len =
-                sqrtf(sumsq3(__fsub_rn(p1[0], p0[0]), __fsub_rn(p1[1], p0[1]), __fsub_rn(p1[2], p0[2])));
-            if (len >= 1e-9f) {  // ct_projector_3d.cu:137
-                float f[3];
-                world_to_index3(A, __fmul_rn(0.5f, __fadd_rn(p0[0], p1[0])),
-                                __fmul_rn(0.5f, __fadd_rn(p0[1], p1[1])), __fmul_rn(0.5f, __fadd_rn(p0[2], p1[2])),
-                                f[0], f[1], f[2]);
-                const int ii = __float2int_rn(f[0]), jj = __float2int_rn(f[1]), kk = __float2int_rn(f[2]);
-                if (ii >= 0 && ii < D.n[0] && jj >= 0 && jj < D.n[1] && kk >= 0 && kk < D.n[2]) {
-                    const int v = (ii * D.n[1] + jj) * D.n[2] + kk;
-                    if constexpr (ADJ) atomicAdd(vout + v, __fmul_rn(y, len));
-                    else acc = __fmaf_rn(__ldg(vol + v), len, acc);
-                }
+        for (int a = 0; a < 3; ++a) p1[a] = __fmaf_rn(t1, vw[a], sw[a]);
+        const float len = sqrtf(sumsq3(__fsub_rn(p1[0], p0[0]), __fsub_rn(p1[1], p0[1]), __fsub_rn(p1[2], p0[2])));
+        if (len >= 1e-9f) {  // ct_projector_3d.cu:137
+            float f[3];
+            world_to_index3(A, __fmul_rn(0.5f, __fadd_rn(p0[0], p1[0])), __fmul_rn(0.5f, __fadd_rn(p0[1], p1[1])),
+                            __fmul_rn(0.5f, __fadd_rn(p0[2], p1[2])), f[0], f[1], f[2]);
+            const int ii = __float2int_rn(f[0]), jj = __float2int_rn(f[1]), kk = __float2int_rn(f[2]);
+            if ((unsigned)ii < (unsigned)D.n[0] && (unsigned)jj < (unsigned)D.n[1] && (unsigned)kk < (unsigned)D.n[2]) {
+                const int v = (ii * D.n[1] + jj) * D.n[2] + kk;
+                if constexpr (ADJ) atomicAdd(vout + v, __fmul_rn(y, len));
+                else acc = __fmaf_rn(__ldg(vol + v), len, acc);
             }
         }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p0[a] = p1[a];
     }
-    if constexpr (!ADJ) {
-        acc = warp_sum(acc);
-        if (lane == 0) out[bi * n_ray + r] = acc;
-    }
+    if constexpr (!ADJ) out[bi * n_ray + r] = acc;
 }
 
 // ----------------------------------------------------------------------------
@@ -470,6 +454,18 @@ static int check_grid(const char* what, int ndim, const int64_t* dims, Dims& D, 
     return CTLAB_OK;
 }
 
+constexpr int kLaneThreads = 128;
+
+// One thread per ray, kLaneThreads per block.
+static int lane_grid(const char* what, int64_t n_ray, int64_t batch, dim3& grid) {
+    CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
+    CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535]", what);
+    const int64_t blocks = (n_ray + kLaneThreads - 1) / kLaneThreads;
+    CTLAB_REQUIRE(blocks <= kMaxGrid, "%s: too many rays", what);
+    grid = dim3((unsigned)blocks, (unsigned)batch);
+    return CTLAB_OK;
+}
+
 static int warp_grid(const char* what, int64_t n_ray, int64_t batch, dim3& grid) {
     CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535]", what);
@@ -488,7 +484,7 @@ static int run_tvals(const char* what, const float* in, float* out, int64_t batc
     int rc = check_grid(what, NDIM, dims, D, nvox);
     if (rc) return rc;
     dim3 grid;
-    rc = warp_grid(what, n_ray, batch, grid);
+    rc = lane_grid(what, n_ray, batch, grid);
     if (rc) return rc;
     CTLAB_REQUIRE(n_int >= 1 && n_int < (1LL << 30), "%s: n_int out of range", what);
     CTLAB_REQUIRE((ADJ ? out : in) && M_inv && b, "%s: null data pointer", what);
@@ -496,8 +492,8 @@ static int run_tvals(const char* what, const float* in, float* out, int64_t batc
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (n_ray == 0) return CTLAB_OK;
-    tvals_kernel<NDIM, ADJ><<<grid, 32 * kWarpsPerBlock, 0, s>>>(in, out, tvals, (int)n_int, src, dst, n_ray, M_inv,
-                                                                 b, D, nvox);
+    tvals_lane_kernel<NDIM, ADJ><<<grid, kLaneThreads, 0, s>>>(in, out, tvals, (int)n_int, src, dst, n_ray, M_inv, b,
+                                                               D, nvox);
     return launch_status(what);
 }
 
@@ -511,7 +507,7 @@ static int run_compressed(const char* what, const float* in, float* out, int64_t
     int rc = check_grid(what, 3, dims, D, nvox);
     if (rc) return rc;
     dim3 grid;
-    rc = warp_grid(what, n_ray, batch, grid);
+    rc = lane_grid(what, n_ray, batch, grid);
     if (rc) return rc;
     CTLAB_REQUIRE(n_int >= 1 && n_int < (1LL << 30), "%s: n_int out of range", what);
     CTLAB_REQUIRE((ADJ ? out : in) && M_inv && b, "%s: null data pointer", what);
@@ -520,8 +516,8 @@ static int run_compressed(const char* what, const float* in, float* out, int64_t
     cudaStream_t s = as_stream(stream);
     if (ADJ && !accumulate) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * nvox), s));
     if (n_ray == 0) return CTLAB_OK;
-    compressed_kernel<ADJ><<<grid, 32 * kWarpsPerBlock, 0, s>>>(in, out, tq, t_start, t_scale, (int)n_int, src, dst,
-                                                                n_ray, M_inv, b, D, nvox);
+    compressed_lane_kernel<ADJ><<<grid, kLaneThreads, 0, s>>>(in, out, tq, t_start, t_scale, (int)n_int, src, dst,
+                                                              n_ray, M_inv, b, D, nvox);
     return launch_status(what);
 }
 

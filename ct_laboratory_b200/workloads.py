@@ -24,7 +24,7 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
-__all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "ServingWorkload", "WORKLOADS"]
+__all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "ServingWorkload", "StaticRingWorkload", "WORKLOADS"]
 
 
 @dataclass(frozen=True)
@@ -181,5 +181,65 @@ class ServingWorkload:
         return out
 
 
+@dataclass(frozen=True)
+class StaticRingWorkload:
+    """A StaticCT ring the size of the reference's published benchmark scan
+    (80 sources x 3 gantry rotations = 240 views, 16 active modules of 48 x 16
+    cells per source = 12,288 cells per view, 2,949,120 rays; 512^2 x 64 voxels
+    over a 400 mm x 60 mm field shifted 5 mm in z).  The calibrated geometry
+    file behind the published numbers is not available, so the ring is the
+    uniform one: 48 modules on a 400 mm radius, sources on a 420 mm radius,
+    1.0 x 4.0 mm cells, rotations of 0, 1.5 and 3 degrees."""
+    name: str = "static512"
+    n: tuple = (512, 512, 64)
+    fov_xy: float = 400.0
+    fov_z: float = 60.0
+    z_shift: float = 5.0
+    n_source: int = 80
+    source_radius: float = 420.0
+    n_module: int = 48
+    module_radius: float = 400.0
+    det_nx: int = 48
+    det_ny: int = 16
+    pitch_x: float = 1.0
+    pitch_y: float = 4.0
+    modules_per_source: int = 16
+    rotations_deg: tuple = (0.0, 1.5, 3.0)
+    n_ellipsoid: int = 12
+    seed: int = 0
+
+    @property
+    def n_ray(self):
+        return self.n_source * len(self.rotations_deg) * self.modules_per_source * self.det_nx * self.det_ny
+
+    @property
+    def voxel(self):
+        return (self.fov_xy / self.n[0], self.fov_xy / self.n[1], self.fov_z / self.n[2])
+
+    def projector(self, device):
+        import math
+
+        import torch
+
+        from .tomography import UniformStaticCTProjector3D, standard_image_transform_3d
+        M, b = standard_image_transform_3d(*self.n, *self.voxel)
+        b = b + torch.tensor([0.0, 0.0, self.z_shift])
+        rots = []
+        for deg in self.rotations_deg:
+            c, s = math.cos(math.radians(deg)), math.sin(math.radians(deg))
+            rots.append(torch.tensor([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]], dtype=torch.float32))
+        Mg = torch.stack(rots)
+        bg = torch.zeros(len(rots), 3)
+        act = torch.ones(len(rots), self.n_source, dtype=torch.bool)
+        return UniformStaticCTProjector3D(*self.n, self.n_source, self.source_radius, 0.0, self.n_module,
+                                          self.module_radius, self.det_nx, self.det_ny, self.pitch_x, self.pitch_y,
+                                          0.0, Mg, bg, act, self.modules_per_source, M, b, device=device)
+
+    def phantom(self, device="cpu"):
+        from .phantoms import ellipsoid_phantom_3d
+        return ellipsoid_phantom_3d(*self.n, voxel=self.voxel[0], n_ellipsoid=self.n_ellipsoid, seed=self.seed,
+                                    device=device)
+
+
 WORKLOADS = {"cone256": ConeWorkload(), "fan256": FanWorkload(), "batch64": ScanBatchWorkload(),
-             "serve": ServingWorkload()}
+             "serve": ServingWorkload(), "static512": StaticRingWorkload()}
