@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) add_transposed_kernel(float* __restrict__
 
 // blockIdx.y covers batch items NB at a time: the walk of a tile is done once
 // for NB volumes (a batch of B volumes costs B / NB walks, not B).
-template <bool ADJ, int NB>
+template <bool ADJ, int NB, int W = 32>
 __global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
     siddon3d_shared_xy_kernel(const float* __restrict__ in, float* __restrict__ out, const float* __restrict__ src,
                               const float* __restrict__ dst, int64_t n_ray, const float* __restrict__ M_inv,
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
     const Affine3 A = load_affine3(M_inv, bvec);
     const int64_t b0 = (int64_t)blockIdx.y * NB;
     const int nb = min(NB, batch - (int)b0);
-    shared_xy_ray<ADJ, NB>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), b0, nb, cells[threadIdx.x >> 5]);
+    shared_xy_ray<ADJ, NB, W>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), b0, nb, cells[threadIdx.x >> 5]);
 }
 
 
@@ -125,11 +125,18 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
         // crossing rule take the shared x-y walk; it checks per warp that the
         // lanes share their x-y line and otherwise runs the per-lane walk.
         const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
-        if (!flat && !mid && small_grid && T.tile_rows % 32 == 0 &&
+        if (!flat && !mid && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
             (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
             const int nb = batch >= 4 ? 4 : (batch >= 2 ? 2 : 1);
             const dim3 g((unsigned)T.n_blocks, (unsigned)((batch + nb - 1) / nb));
             const int bt = (int)batch;
+            if (T.tile_rows == 16) {
+                // 16 detector rows per column: two 16-lane groups per warp, one volume per walk
+                const dim3 g1((unsigned)T.n_blocks, (unsigned)batch);
+                siddon3d_shared_xy_kernel<ADJ, 1, 16>
+                    <<<g1, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+                return launch_status(what);
+            }
             if (nb == 4)
                 siddon3d_shared_xy_kernel<ADJ, 4><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
             else if (nb == 2)

@@ -861,16 +861,18 @@ __device__ __forceinline__ int slab_at(float t, float s, float va, float inv, in
 
 // Number of lanes m whose `sorted` value (non-decreasing over the lanes) is
 // below `key` (INCLUSIVE: at or below): a branch-free binary search.
-template <bool INCLUSIVE>
+// W: the lanes searched are the caller's group of W lanes (W = 32: the warp;
+// W = 16: its half), lane indices relative to the group.
+template <bool INCLUSIVE, int W = 32>
 __device__ __forceinline__ int warp_rank(float sorted, float key) {
     int c = 0;
 #pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-        const float v = __shfl_sync(kFullMask, sorted, c + step - 1);
+    for (int step = W / 2; step > 0; step >>= 1) {
+        const float v = __shfl_sync(kFullMask, sorted, c + step - 1, W);
         c += (INCLUSIVE ? v <= key : v < key) ? step : 0;
     }
-    // c counts lanes 0..30; lane 31 is the one left to test
-    const float v = __shfl_sync(kFullMask, sorted, c);
+    // c counts lanes 0..W-2; lane W-1 is the one left to test
+    const float v = __shfl_sync(kFullMask, sorted, c, W);
     return c + ((INCLUSIVE ? v <= key : v < key) ? 1 : 0);
 }
 
@@ -944,12 +946,24 @@ __device__ __forceinline__ float accumulate_group(const CellGroup<NG>& g, const 
 // from (forward) or reduces into (adjoint) all nb volumes.  All 32 lanes of
 // the warp call it together; `buf` is the warp's kChunk-entry shared-memory
 // cell buffer.
-template <bool ADJ, int NB>
+//
+// W = 16 splits the warp into two groups of 16 lanes, each walking its own
+// x-y line with 16 crossings per round (detectors with 16 rows per column,
+// such as StaticCT modules, tiled 16 rows x 2 columns per warp).  The two
+// groups keep step round by round (the rank search shuffles within each
+// half, with all 32 lanes taking part), a group that has left the volume
+// idling until the other is done; every decision that branches around a
+// collective step is taken for the whole warp.
+template <bool ADJ, int NB, int W = 32>
 __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, float* __restrict__ out,
                                               const float* __restrict__ src, const float* __restrict__ dst,
                                               int64_t n_ray, const Affine3& A, const GridDims<3>& G,
                                               int64_t nvox, int64_t r, int64_t b0, int nb, XYCell* buf) {
-    const int lane = threadIdx.x & 31;
+    static_assert(W == 32 || W == 16, "group width must be 32 or 16");
+    const int wlane = threadIdx.x & 31;
+    const int lane = wlane & (W - 1);  // lane within the group
+    const unsigned gmask = W == 32 ? kFullMask : (0xffffu << (wlane & 16));
+    buf += wlane & (32 - W);  // the group's part of the warp's buffer
     float sw[3] = {0.f, 0.f, 0.f}, dw[3] = {0.f, 0.f, 0.f};
     if (r >= 0) {
 #pragma unroll
@@ -972,8 +986,9 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     lane_setup(R, sw, dw, G, A);
     R.live = R.live && (r >= 0) && (!ADJ || any_y);
 
-    const unsigned live_mask = __ballot_sync(kFullMask, R.live);
-    if (live_mask == 0u) {
+    const unsigned warp_live = __ballot_sync(kFullMask, R.live);
+    const unsigned live_mask = warp_live & gmask;
+    if (warp_live == 0u) {
         if (!ADJ && r >= 0) {
 #pragma unroll
             for (int j = 0; j < NB; ++j)
@@ -983,7 +998,8 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     }
     // Do the live lanes share their x-y line, and is every live lane's z
     // slope inside the one-z-plane-per-cell bound?  (Dead lanes do not vote.)
-    const int leader = __ffs(live_mask) - 1;
+    // (a group without live lanes reads its first lane; nothing it walks has length)
+    const int leader = live_mask ? __ffs(live_mask) - 1 : (wlane & (32 - W));
     const float s0 = __shfl_sync(kFullMask, R.s[0], leader), s1 = __shfl_sync(kFullMask, R.s[1], leader);
     const float va0 = __shfl_sync(kFullMask, R.va[0], leader), va1 = __shfl_sync(kFullMask, R.va[1], leader);
     const float i0 = __shfl_sync(kFullMask, R.inv[0], leader), i1 = __shfl_sync(kFullMask, R.inv[1], leader);
@@ -994,7 +1010,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
                                 __float_as_uint(R.va[1]) == __float_as_uint(va1) &&
                                 fabsf(R.va[2]) <= 0.75f * vxy && fabsf(R.s[0]) <= 131072.f &&
                                 fabsf(R.s[1]) <= 131072.f && fabsf(R.s[2]) <= 131072.f);
-    if (!__all_sync(kFullMask, ok) || vxy == 0.f) {
+    if (!__all_sync(kFullMask, ok && (live_mask == 0u || vxy != 0.f))) {
         if (r < 0) return;
 #pragma unroll 1
         for (int j = 0; j < nb; ++j) {  // the per-lane walk, once per volume
@@ -1016,7 +1032,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     const float kInf = __int_as_float(0x7f800000);
     float t_start = R.live ? R.t_enter : kInf, t_stop = R.live ? R.t_exit : -kInf;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = W / 2; o > 0; o >>= 1) {
         t_start = fminf(t_start, __shfl_xor_sync(kFullMask, t_start, o));
         t_stop = fmaxf(t_stop, __shfl_xor_sync(kFullMask, t_stop, o));
     }
@@ -1090,7 +1106,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     }
     const uint64_t pol = l2_policy_keep();
     const float fl = (float)lane;
-    const int max_rounds = (G.n[0] + G.n[1] + 2) / kChunk + 2;
+    const int max_rounds = (G.n[0] + G.n[1] + 2) / W + 2;
     // forward: cells per step so that every step has 2 * kGroupFwd gathers in flight
     constexpr int kGF = kGroupFwd / NB > 0 ? kGroupFwd / NB : 1;
     // Do all 32 lanes trace live rays entering and leaving at the warp's
@@ -1099,6 +1115,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
     auto rounds = [&](auto uni_tag) {
         constexpr bool UNI = decltype(uni_tag)::value;
+        bool fin = false;  // W = 16: this group has walked its last cell
 #pragma unroll 1
         for (int round = 0; round < max_rounds; ++round) {
             // lane l: the l-th next x plane and the l-th next y plane (plane
@@ -1106,19 +1123,19 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
             float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
             float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
             // merged positions; on equal parameters the x crossing comes first
-            const int rx = lane + warp_rank<false>(ty, tx);
-            const int ry = lane + warp_rank<true>(tx, ty);
+            const int rx = lane + warp_rank<false, W>(ty, tx);
+            const int ry = lane + warp_rank<true, W>(tx, ty);
             if (UNI) {  // cell ends past the common exit are the exit
                 tx = fminf(tx, t_stop);
                 ty = fminf(ty, t_stop);
             }
-            if (rx < kChunk) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
-            if (ry < kChunk) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
-            const int n_x = __popc(__ballot_sync(kFullMask, rx < kChunk));
+            if (rx < W) buf[rx] = XYCell{tx, col + lane * dsx + (rx - lane) * dsy};
+            if (ry < W) buf[ry] = XYCell{ty, col + (ry - lane) * dsx + lane * dsy};
+            const int n_x = __popc(__ballot_sync(kFullMask, rx < W) & gmask);
             __syncwarp();
             // cells up to and including the one that ends at or after t_stop
-            const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop));
-            const int n_cells = min(n_in + 1, kChunk);
+            const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop) & gmask);
+            const int n_cells = (W == 16 && fin) ? 0 : min(n_in + 1, W);
             if constexpr (ADJ) {
                 // y * |v| once per lane, times each parameter span: the same
                 // segment lengths as the forward's, multiplied in another order
@@ -1150,11 +1167,18 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
                     for (int j = 0; j < NB; ++j) acc[j] = accumulate_group<kGF>(g, v[j], acc[j]);
                 }
             }
-            if (n_in < kChunk) break;
+            if constexpr (W == 32) {
+                if (n_in < W) break;
+            } else {
+                fin = fin || n_in < W;
+                if (__all_sync(kFullMask, fin)) break;
+            }
             __syncwarp();  // every lane is done with this round's cells
-            col += n_x * dsx + (kChunk - n_x) * dsy;
-            pnx = __fmaf_rn((float)n_x, psx, pnx);
-            pny = __fmaf_rn((float)(kChunk - n_x), psy, pny);
+            if (W == 32 || !fin) {
+                col += n_x * dsx + (W - n_x) * dsy;
+                pnx = __fmaf_rn((float)n_x, psx, pnx);
+                pny = __fmaf_rn((float)(W - n_x), psy, pny);
+            }
         }
     };
 #if CTLAB_XY_UNIFORM

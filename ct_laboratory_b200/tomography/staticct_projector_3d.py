@@ -14,9 +14,11 @@ from typing import Optional
 
 import torch
 
+from .. import _native as N
 from .ct_projector_3d_module import CTProjector3DModule
 
 __all__ = ["build_circular_sequence", "build_helical_sequence", "build_static_3d_geometry", "StaticCTProjector3D",
+           "staticct_ray_tiling",
            "build_uniform_static_3d_geometry", "UniformStaticCTProjector3D"]
 
 
@@ -142,13 +144,29 @@ def build_uniform_static_3d_geometry(n_source, source_radius, source_z_offset, n
     return sp, mc, mo, mask
 
 
+def staticct_ray_tiling(n_view, det_nx_per_module, det_ny_per_module, voxel_rule=1, block_threads=128):
+    """Launch tiling for StaticCT rays ordered [view][column][row] per module
+    (the order build_static_3d_geometry emits: for each active (frame,
+    source, module) the module's columns, rows fastest), n_view = the number
+    of (frame, source, module) triples.  The lanes of a warp run down module
+    rows, which share one x-y line from the source: with 16 rows per column
+    two 16-lane groups per warp take the column walk, with a multiple of 32
+    rows whole warps do.  Other row counts get None (flat launch)."""
+    if det_ny_per_module != 16 and det_ny_per_module % 32 != 0:
+        return None
+    rows = 16 if det_ny_per_module == 16 else 32
+    per = det_nx_per_module * det_ny_per_module
+    return N.tiling(n_view, det_ny_per_module, det_nx_per_module, per, 1, det_ny_per_module, tile_rows=rows,
+                    block_threads=block_threads, voxel_rule=voxel_rule)
+
+
 class UniformStaticCTProjector3D(StaticCTProjector3D):
     """Reference staticct_projector_3d.py:460-539."""
 
     def __init__(self, n_x, n_y, n_z, n_source, source_radius, source_z_offset, n_module, module_radius,
                  det_nx_per_module, det_ny_per_module, det_spacing_x, det_spacing_y, module_z_offset, M_gantry,
                  b_gantry, active_sources, modules_per_source, M, b, backend="cuda", precomputed_intersections=False,
-                 tvals=None, use_compression=True, device: Optional[torch.device] = None):
+                 tvals=None, use_compression=True, device: Optional[torch.device] = None, ray_tiling=None):
         if device is None:
             device = torch.device("cuda" if backend == "cuda" and torch.cuda.is_available() else "cpu")
         sp, mc, mo, smm = build_uniform_static_3d_geometry(n_source=n_source, source_radius=source_radius,
@@ -162,4 +180,4 @@ class UniformStaticCTProjector3D(StaticCTProjector3D):
                          det_spacing_x=det_spacing_x, det_spacing_y=det_spacing_y, source_module_mask=smm,
                          active_sources=active_sources.to(device), M=M.to(device), b=b.to(device), backend=backend,
                          precomputed_intersections=precomputed_intersections, tvals=tvals,
-                         use_compression=use_compression, device=device)
+                         use_compression=use_compression, device=device, ray_tiling=ray_tiling)

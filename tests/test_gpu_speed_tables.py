@@ -11,8 +11,10 @@ grid.
 
 * Ours, on the whole scan: the float table (compute_intersections_3d), its
   uint16 compression with the reference CUDA encoder, forward / adjoint from
-  the compressed and from the float table, and the on-the-fly walk under
-  both voxel rules for comparison.
+  the compressed and from the float table, and the on-the-fly walk for
+  comparison: both voxel rules flat, and the crossing rule with the modules'
+  16 rows per column tiled for the column walk (forward bitwise equal to
+  the flat walk's).
 * The reference's kernels (compiled from its sources into oracle/_ref), on
   every tenth view: table, compression, forward / adjoint from both tables.
   A ray's cost does not depend on the other rays, so rays per second on the
@@ -77,6 +79,7 @@ def _once_ms(fn):
 def test_static512_table_paths_vs_reference(ref):
     from ct_laboratory_b200 import _C
     from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.tomography import staticct_ray_tiling
     from ct_laboratory_b200.tomography._common import voxel_diag_len
     from ct_laboratory_b200.workloads import WORKLOADS
     w = WORKLOADS["static512"]
@@ -105,6 +108,9 @@ def test_static512_table_paths_vs_reference(ref):
             _ms(lambda: _C.forward_project_3d_compressed_cuda(x, u16, st, sc, src, dst, Mi, b), flush=flush),
             _ms(lambda: _C.back_project_3d_compressed_cuda(y, u16, st, sc, src, dst, Mi, b, nx, ny, nz), flush=flush)]
         cross = N.flat_opts(voxel_rule=N.VOXEL_CROSSING, block_threads=128)
+        col16 = staticct_ray_tiling(n_ray // (w.det_nx * w.det_ny), w.det_nx, w.det_ny, voxel_rule=N.VOXEL_CROSSING)
+        assert torch.equal(_C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=col16),
+                           _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=cross))
         res["ours_on_the_fly_ms"] = {
             "midpoint": [_ms(lambda: _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b), flush=flush),
                          _ms(lambda: _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, nx, ny, nz),
@@ -112,7 +118,11 @@ def test_static512_table_paths_vs_reference(ref):
             "crossing": [_ms(lambda: _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=cross),
                              flush=flush),
                          _ms(lambda: _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, nx, ny, nz, tiling=cross),
-                             flush=flush)]}
+                             flush=flush)],
+            "crossing_column_walk": [
+                _ms(lambda: _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=col16), flush=flush),
+                _ms(lambda: _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, nx, ny, nz, tiling=col16),
+                    flush=flush)]}
 
         # ---- the sample of whole views
         per_view = w.modules_per_source * w.det_nx * w.det_ny
