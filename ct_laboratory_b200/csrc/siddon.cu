@@ -131,10 +131,13 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
             const dim3 g((unsigned)T.n_blocks, (unsigned)((batch + nb - 1) / nb));
             const int bt = (int)batch;
             if (T.tile_rows == 16) {
-                // 16 detector rows per column: two 16-lane groups per warp, one volume per walk
-                const dim3 g1((unsigned)T.n_blocks, (unsigned)batch);
-                siddon3d_shared_xy_kernel<ADJ, 1, 16>
-                    <<<g1, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+                // 16 detector rows per column: two 16-lane groups per warp
+                if (nb == 4)
+                    siddon3d_shared_xy_kernel<ADJ, 4, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+                else if (nb == 2)
+                    siddon3d_shared_xy_kernel<ADJ, 2, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+                else
+                    siddon3d_shared_xy_kernel<ADJ, 1, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
                 return launch_status(what);
             }
             if (nb == 4)

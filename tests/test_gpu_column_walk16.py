@@ -33,7 +33,8 @@ def _ring():
     return p, n, n_frame * n_source * 4
 
 
-def test_two_group_column_walk_equals_per_lane_walk():
+@pytest.mark.parametrize("batch", [1, 3, 5])  # 1, 2 and 4 volumes per walk (and a partial last group)
+def test_two_group_column_walk_equals_per_lane_walk(batch):
     from ct_laboratory_b200 import _C
     from ct_laboratory_b200 import _native as N
     from ct_laboratory_b200.tomography import staticct_ray_tiling
@@ -44,8 +45,8 @@ def test_two_group_column_walk_equals_per_lane_walk():
     assert tiled is not None and tiled.tile_rows == 16
     flat = N.flat_opts(voxel_rule=N.VOXEL_CROSSING, block_threads=128)
     g = torch.Generator(device=DEV).manual_seed(3)
-    x = torch.rand(3, *n, device=DEV, generator=g)
-    y = torch.rand(3, src.shape[0], device=DEV, generator=g)
+    x = torch.rand(batch, *n, device=DEV, generator=g)
+    y = torch.rand(batch, src.shape[0], device=DEV, generator=g)
 
     f16 = _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=tiled)
     f1 = _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=flat)
@@ -60,7 +61,7 @@ def test_two_group_column_walk_equals_per_lane_walk():
 
     b16 = _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, *n, tiling=tiled)
     b1 = _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, *n, tiling=flat)
-    for k in range(3):
+    for k in range(batch):
         assert rel_err(b16[k].cpu().numpy(), b1[k].cpu().numpy()) < TOL
 
 
