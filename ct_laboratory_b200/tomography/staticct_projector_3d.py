@@ -166,9 +166,18 @@ class UniformStaticCTProjector3D(StaticCTProjector3D):
     def __init__(self, n_x, n_y, n_z, n_source, source_radius, source_z_offset, n_module, module_radius,
                  det_nx_per_module, det_ny_per_module, det_spacing_x, det_spacing_y, module_z_offset, M_gantry,
                  b_gantry, active_sources, modules_per_source, M, b, backend="cuda", precomputed_intersections=False,
-                 tvals=None, use_compression=True, device: Optional[torch.device] = None, ray_tiling=None):
+                 tvals=None, use_compression=True, device: Optional[torch.device] = None, ray_tiling=None,
+                 voxel_rule=0):
+        """voxel_rule 0 is the reference's midpoint rule; 1, the crossing
+        rule, also tiles the rays for the column walk (staticct_ray_tiling)
+        unless a ray_tiling is given."""
         if device is None:
             device = torch.device("cuda" if backend == "cuda" and torch.cuda.is_available() else "cpu")
+        if ray_tiling is None and voxel_rule == N.VOXEL_CROSSING:
+            n_view = int(torch.as_tensor(active_sources).sum()) * int(modules_per_source)
+            ray_tiling = staticct_ray_tiling(n_view, det_nx_per_module, det_ny_per_module, voxel_rule=voxel_rule)
+            if ray_tiling is None:
+                ray_tiling = N.flat_opts(voxel_rule=voxel_rule, block_threads=128)
         sp, mc, mo, smm = build_uniform_static_3d_geometry(n_source=n_source, source_radius=source_radius,
                                                            source_z_offset=source_z_offset, n_module=n_module,
                                                            module_radius=module_radius,

@@ -79,6 +79,9 @@ def test_static_module_takes_the_tiling():
                                ray_tiling=N.flat_opts(voxel_rule=N.VOXEL_CROSSING))
     x = torch.rand(*n, device=DEV, requires_grad=True)
     assert torch.equal(tiled(x), flat(x))
+    auto = UniformStaticCTProjector3D(*n, 6, 60.0, 0.0, 12, 55.0, 8, 16, 3.0, 1.5, 0.0, p.M_gantry, p.b_gantry,
+                                      p.active_sources, 4, p.M, p.b, device=torch.device(DEV), voxel_rule=1)
+    assert auto.ray_tiling.tile_rows == 16 and torch.equal(auto(x), flat(x))
     yv = torch.rand(p.src.shape[0], device=DEV)
     (tiled(x) * yv).sum().backward()
     assert rel_err(x.grad.cpu().numpy(), flat.back_project(yv).cpu().numpy()) < TOL
