@@ -20,8 +20,8 @@ time is the max over ranks.  Rank 0 prints one JSON line that also holds:
                 host's cores, on a bounded sample of views (N = 1 only)
   e2e           the same metric through the public module API with pinned
                 host buffers, H2D of each step's inputs and D2H of its outputs
-                inside the timed region (copies on a second stream, under
-                the kernels)
+                inside the timed region (inputs double-buffered, uploads and
+                downloads each on a stream of its own, under the kernels)
   clocks        nvidia-smi SM clock / throttle reasons sampled while timing
 and, at N = 1, three legs of the other workloads (each can be switched off):
   batched       64 uneven 2-D scans: one persistent launch per direction from
