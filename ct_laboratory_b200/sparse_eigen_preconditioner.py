@@ -154,9 +154,10 @@ class SparseEigenDecomposition(nn.Module):
                        use_tqdm=False, **_ignored):
         """Thick-restart Lanczos for the k largest eigenpairs, on the device.
 
-        Basis V (N x (ncv+1)) in float32 with two passes of classical
-        Gram-Schmidt against all previous vectors per step; the projected
-        matrix T = V^T G V in float64.  After ncv vectors the k leading Ritz
+        Basis V ((ncv+1) x N, one vector per row, so that every product with
+        it reads whole contiguous vectors) in float32 with two passes of
+        classical Gram-Schmidt against all previous vectors per step; the
+        projected matrix T = V G V^T in float64.  After ncv vectors the k leading Ritz
         vectors and the residual direction are kept and the iteration
         continues from them (thick restart).  Converged when every kept Ritz
         pair has residual |beta * s_last| <= tol * theta_max."""
@@ -165,26 +166,26 @@ class SparseEigenDecomposition(nn.Module):
         if not (k < ncv < N):
             raise ValueError("lanczos needs k < ncv < N")
         gen = torch.Generator(device="cpu").manual_seed(int(seed))
-        V = torch.empty(N, ncv + 1, dtype=dt, device=dev)
+        V = torch.empty(ncv + 1, N, dtype=dt, device=dev)
         v0 = torch.randn(N, generator=gen, dtype=dt).to(dev)
-        V[:, 0] = v0 / v0.norm()
+        V[0] = v0 / v0.norm()
         T = torch.zeros(ncv, ncv, dtype=torch.float64, device=dev)
         start = 0
         beta_last = 0.0
         for restart in range(int(max_restarts)):
             for j in range(start, ncv):
-                w = self._apply_gram(V[:, j])
-                h = V[:, :j + 1].t() @ w
-                w = w - V[:, :j + 1] @ h
-                h2 = V[:, :j + 1].t() @ w
-                w = w - V[:, :j + 1] @ h2
+                w = self._apply_gram(V[j])
+                h = V[:j + 1] @ w
+                w = w - V[:j + 1].t() @ h
+                h2 = V[:j + 1] @ w
+                w = w - V[:j + 1].t() @ h2
                 h = (h + h2).double()
                 T[:j + 1, j] = h
                 T[j, :j + 1] = h
                 beta = w.norm()
                 if j + 1 < ncv:
                     T[j + 1, j] = T[j, j + 1] = beta.double()
-                V[:, j + 1] = w / beta.clamp_min(1e-30)
+                V[j + 1] = w / beta.clamp_min(1e-30)
                 beta_last = beta
             theta, S = torch.linalg.eigh(T)
             order = torch.argsort(theta, descending=True)
@@ -196,17 +197,17 @@ class SparseEigenDecomposition(nn.Module):
             if bool((res <= tol * theta[0].abs()).all()) or restart == max_restarts - 1:
                 break
             # thick restart: keep k Ritz vectors and the residual direction
-            Y = V[:, :ncv] @ S[:, :k].to(dt)
-            resid = V[:, ncv].clone()
-            V[:, :k] = Y
-            V[:, k] = resid
+            Y = S[:, :k].t().to(dt) @ V[:ncv]
+            resid = V[ncv].clone()
+            V[:k] = Y
+            V[k] = resid
             T.zero_()
             T[:k, :k] = torch.diag(theta[:k])
             coup = beta_last.double() * S[-1, :k]
             T[k, :k] = coup
             T[:k, k] = coup
             start = k
-        Y = V[:, :ncv] @ S[:, :k].to(dt)
+        Y = (S[:, :k].t().to(dt) @ V[:ncv]).t()
         return torch.clamp(theta[:k], min=0.0).to(dt), Y
 
     # -- public API --------------------------------------------------------------
