@@ -85,20 +85,24 @@ def tile_kinds(p):
     col32     3-D detector grid: 32 detector rows x (block_threads/32) columns
               (lanes of a warp down one detector column: the column walk)
     col64     3-D: 64 rows x (block_threads/64) columns
+    col16     3-D detector grid of 16 rows per column (StaticCT modules):
+              16 rows x (block_threads/16) columns, the column walk in two
+              16-lane groups per warp
     """
     kinds = ["flat"]
     if _ndim(p) == 2:
         if _ray_grid(p) is not None:
             kinds += ["grid32", "grid64", "vgrid32", "vgrid64"]
     elif getattr(p, "ray_tiling", None) is not None and p.ray_tiling.n_view > 0:
-        kinds += ["col32", "col64"]
+        kinds += ["col16"] if p.ray_tiling.n_row == 16 else ["col32", "col64"]
     return kinds
 
 
 def _opts(p, kind, voxel_rule, block_threads):
     """RayOpts of projector p laid out as `kind` (falls back to flat when the
     kind does not apply or does not fit block_threads)."""
-    rows = {"grid32": 32, "grid64": 64, "vgrid32": 32, "vgrid64": 64, "col32": 32, "col64": 64}.get(kind)
+    rows = {"grid32": 32, "grid64": 64, "vgrid32": 32, "vgrid64": 64, "col32": 32, "col64": 64,
+            "col16": 16}.get(kind)
     if rows is None or rows > block_threads or kind not in tile_kinds(p):
         return N.flat_opts(voxel_rule=voxel_rule, block_threads=block_threads)
     if kind.startswith("grid"):
@@ -216,7 +220,9 @@ class ScanBatch:
         out = []
         for p in self.projectors:
             k = tile_kinds(p)
-            if "col32" in k:
+            if "col16" in k:
+                out.append("col16")
+            elif "col32" in k:
                 out.append("col32")
             elif "grid32" in k:
                 out.append("grid32")
@@ -227,7 +233,7 @@ class ScanBatch:
     def configure(self, block_threads=256, kind="auto", n_cta=0, direction="both", mode="auto"):
         """(Re)plan the batch with a tile layout: `kind` is one tile kind for
         every scan or a list with one kind per scan; "auto" takes col32 for
-        detector grids in 3-D, grid32 for 2-D view x cell grids (neighbouring
+        detector grids in 3-D (col16 for 16 rows per column), grid32 for 2-D view x cell grids (neighbouring
         rays in a warp: coherent gathers, and adjoint reductions into
         neighbouring pixels of one row), else flat.  `direction` ("fwd", "adj" or "both")
         selects the plan(s) to replace.  `mode` is how forward() / back() run

@@ -136,6 +136,11 @@ __global__ void __launch_bounds__(256, (NDIM == 3 && !ADJ) ? CTLAB_BATCH_MIN_BLO
             const Affine3 A = load_affine3(S->M_inv, S->b);
             if constexpr (MID) {
                 if (r >= 0) lane_ray<3, ADJ, true>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0);
+            } else if (ADJ && T.tile_rows == 16) {
+                // 16 rows per column (a warp-uniform branch: one scan per warp).  The
+                // adjoint only: the forward with both walks inlined spills; a batch's
+                // 3-D forward runs scan by scan by default, on the single-scan kernels.
+                shared_xy_ray<ADJ, 1, 16>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0, 1, buf);
             } else {
                 shared_xy_ray<ADJ, 1>(in, out, S->src, S->dst, n_ray, A, G, nvox, r, 0, 1, buf);
             }

@@ -106,6 +106,41 @@ def test_batched_3d_equals_per_scan_loop(kind):
     _check_against_loop(batch)
 
 
+def uneven_static_3d():
+    """StaticCT rings (16 rows per module column, crossing rule: col16 tiles)
+    of uneven grid, source count and module width."""
+    from ct_laboratory_b200.tomography import UniformStaticCTProjector3D, standard_image_transform_3d
+    out = []
+    for n, n_source, n_cols, n_frame in (((32, 28, 12), 5, 8, 2), ((24, 24, 16), 7, 4, 1), ((20, 30, 10), 4, 6, 3)):
+        M, b = standard_image_transform_3d(*n, 1.0, 1.0, 0.5)
+        Mg = torch.stack([_rot3(0.2 * f) for f in range(n_frame)])
+        act = torch.ones(n_frame, n_source, dtype=torch.bool)
+        out.append(UniformStaticCTProjector3D(*n, n_source, 60.0, 0.0, 12, 55.0, n_cols, 16, 3.0, 1.0, 0.0, Mg,
+                                              torch.zeros(n_frame, 3), act, 4, M, b, device=torch.device(DEV),
+                                              voxel_rule=1))
+    return out
+
+
+def _rot3(theta):
+    c, s = math.cos(theta), math.sin(theta)
+    return torch.tensor([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]], dtype=torch.float32)
+
+
+@pytest.mark.parametrize("mode", ["auto", "persistent"])
+def test_batched_static_rings_col16(mode):
+    """16-row detector columns: the persistent adjoint's two-group column walk
+    and both forward modes against the per-scan loop."""
+    from ct_laboratory_b200.batched import ScanBatch, tile_kinds
+    projs = uneven_static_3d()
+    assert all("col16" in tile_kinds(p) for p in projs)
+    batch = ScanBatch(projs, block_threads=128)
+    assert batch.config_adj["kind"] == ["col16"] * 3 and batch.config_adj["mode"] == "persistent"
+    if mode == "persistent":
+        batch.configure(block_threads=128, mode="persistent")
+    _fill(batch)
+    _check_against_loop(batch)
+
+
 def test_batched_midpoint_rule_matches_goldens():
     """The reference's golden cases as scans of one batch each (2-D, 3-D), with
     the reference's voxel rule."""
