@@ -337,7 +337,7 @@ def run_ours(args, world, rank, local):
                 "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "segments": seg, "kernels": kern}
 
-    e2e = run_e2e(proj, x, y, args, dev, w) if args.e2e_steps > 0 else None
+    e2e = run_e2e(proj, x, y, args, dev, w, world) if args.e2e_steps > 0 else None
     batched = run_batched(args, dev, flush) if (world == 1 and args.batched_steps > 0) else None
     serving = run_serving(args, dev) if (world == 1 and args.serve_jobs > 0) else None
     map_leg = run_map(args, dev, proj, x, y) if (world == 1 and args.map_iters > 0 and w.name.startswith("cone")) \
@@ -374,7 +374,7 @@ def _fwd3(proj, x):
     return proj.forward_project(x)
 
 
-def run_e2e(proj, x, y, args, dev, w):
+def run_e2e(proj, x, y, args, dev, w, world=1):
     """Public API, host buffers: H2D of the volume and of the adjoint input,
     D2H of the sinogram and of the back-projection, every step.  The device
     inputs are double-buffered and each copy direction has its own stream
@@ -422,6 +422,7 @@ def run_e2e(proj, x, y, args, dev, w):
         for _ in range(2):
             step()
         torch.cuda.synchronize(dev)
+        barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.e2e_steps):
@@ -429,11 +430,13 @@ def run_e2e(proj, x, y, args, dev, w):
         stream.wait_stream(d2h)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / args.e2e_steps
+        barrier(world)
+    # every rank runs its own scan: the job's time is the slowest rank's
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
     n_ray = y.numel()
-    return {"value": n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
-            "h2d_bytes_per_step": int(x_h.numel() * 4 + y_h.numel() * 4),
-            "d2h_bytes_per_step": int(sino_h.numel() * 4 + vol_h.numel() * 4),
+    return {"value": world * n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
+            "h2d_bytes_per_step": int(world * (x_h.numel() * 4 + y_h.numel() * 4)),
+            "d2h_bytes_per_step": int(world * (sino_h.numel() * 4 + vol_h.numel() * 4)),
             "api": ("ConeBeam3DProjector.__call__ + .back_project" if w.name.startswith("cone")
                     else "FanBeam2DProjector.__call__ + .back_project") +
                    ", inputs double-buffered, H2D and D2H each on a stream of its own"}
