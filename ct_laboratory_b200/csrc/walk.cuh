@@ -753,9 +753,11 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
 // Shared x-y walk for detector columns (3-D, crossing rule).
 //
 // When the 32 lanes of a warp trace rays that share their x-y line (one
-// source, one detector column whose cells run along z: cone-beam views and
-// StaticCT rings tiled with 32 detector rows per warp), every x- and y-plane
-// parameter is bitwise the same for all lanes and only the z planes differ.
+// source, one detector column whose cells run along z: cone-beam views tiled
+// with 32 detector rows per warp), every x- and y-plane parameter is bitwise
+// the same for all lanes and only the z planes differ.  (Detectors with 16
+// rows per column, such as StaticCT modules, run the same walk in two
+// 16-lane groups per warp: shared_xy_ray's W below.)
 // The per-lane walk then spends most of its compare / select work deriving
 // the same x-y crossings 32 times over.  Here the warp derives the merged x-y
 // crossing sequence once, 32 crossings per round: lane l evaluates the l-th
