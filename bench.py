@@ -58,6 +58,7 @@ SEGMENTS = {
     "fan256": 45_364_441,
     "cone256": 6_962_229_058,
     "batch64": 3_042_757_788,
+    "static512": 1_784_871_631,
 }
 METRIC = "GRays/s fwd+adj"
 L2_FLUSH_BYTES = 512 << 20
@@ -283,6 +284,9 @@ def run_ours(args, world, rank, local):
                                    det_spacing=w.pitch, voxel_size=w.voxel, device=dev, tile_rows=args.tile_rows,
                                    voxel_rule=args.voxel_rule, walk=args.walk,
                                    deterministic_adjoint=args.deterministic, block_threads=args.block_threads)
+    elif w.name.startswith("static"):
+        # StaticCT ring: under the crossing rule the modules' 16-row columns take the column walk
+        proj = w.projector(dev, voxel_rule=args.voxel_rule)
     else:
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
                                   pixel_size=w.pixel, device=dev)
@@ -294,7 +298,7 @@ def run_ours(args, world, rank, local):
     launches_per_step = 2
 
     def fwd():
-        return proj.forward_project(x) if not w.name.startswith("cone") else _fwd3(proj, x)
+        return _fwd3(proj, x) if w.name.startswith(("cone", "static")) else proj.forward_project(x)
 
     def adj():
         return proj.back_project(y)
@@ -345,8 +349,8 @@ def run_ours(args, world, rank, local):
     cpu = None
     if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
         view0 = None
-        if w.name.startswith("cone"):
-            pv = w.det_nx * w.det_ny
+        if w.name.startswith(("cone", "static")):
+            pv = w.n_ray // w.n_view
             with torch.no_grad():
                 y0 = torch.zeros_like(y)
                 y0[:pv] = y[:pv]
@@ -437,8 +441,7 @@ def run_e2e(proj, x, y, args, dev, w, world=1):
     return {"value": world * n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
             "h2d_bytes_per_step": int(world * (x_h.numel() * 4 + y_h.numel() * 4)),
             "d2h_bytes_per_step": int(world * (sino_h.numel() * 4 + vol_h.numel() * 4)),
-            "api": ("ConeBeam3DProjector.__call__ + .back_project" if w.name.startswith("cone")
-                    else "FanBeam2DProjector.__call__ + .back_project") +
+            "api": f"{type(proj).__name__}.__call__ + .back_project" +
                    ", inputs double-buffered, H2D and D2H each on a stream of its own"}
 
 

@@ -216,7 +216,18 @@ class StaticRingWorkload:
     def voxel(self):
         return (self.fov_xy / self.n[0], self.fov_xy / self.n[1], self.fov_z / self.n[2])
 
-    def projector(self, device):
+    @property
+    def n_view(self):
+        """(rotation, source) pairs, each a contiguous run of rays."""
+        return self.n_source * len(self.rotations_deg)
+
+    def geometry(self):
+        """src, dst, M, b on the host."""
+        import torch
+        p = self.projector(torch.device("cpu"))
+        return p.src, p.dst, p.M, p.b
+
+    def projector(self, device, voxel_rule=0):
         import math
 
         import torch
@@ -233,7 +244,8 @@ class StaticRingWorkload:
         act = torch.ones(len(rots), self.n_source, dtype=torch.bool)
         return UniformStaticCTProjector3D(*self.n, self.n_source, self.source_radius, 0.0, self.n_module,
                                           self.module_radius, self.det_nx, self.det_ny, self.pitch_x, self.pitch_y,
-                                          0.0, Mg, bg, act, self.modules_per_source, M, b, device=device)
+                                          0.0, Mg, bg, act, self.modules_per_source, M, b, device=device,
+                                          voxel_rule=voxel_rule)
 
     def phantom(self, device="cpu"):
         from .phantoms import ellipsoid_phantom_3d
