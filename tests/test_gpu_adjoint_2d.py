@@ -85,6 +85,28 @@ def test_scratch_adjoint_matches_plain_and_oracle(shape, rule):
     assert rel_err(with_t[1].cpu().numpy(), ref) < TOL
 
 
+@pytest.mark.parametrize("shape", [(12, 4100), (4100, 12)])
+def test_scratch_adjoint_beyond_the_major_walk_bound(shape):
+    """Images wider or taller than 4096 pixels are outside the major-axis
+    walk's bound: every ray takes the merge walk into the image itself, the
+    scratch being zeroed and added back empty."""
+    from ct_laboratory_b200.tomography._common import inverse
+    n_row, n_col = shape
+    n_view, n_det = 16, 64
+    src, dst, M, b = _fan(n_row, n_col, n_view, n_det, pixel=0.05)
+    Mi = inverse(M)
+    for rule in (1, 0):
+        opts = _crossing_opts(n_view, n_det, rule)
+        sino = torch.rand(1, n_view * n_det, device=DEV, generator=torch.Generator(device=DEV).manual_seed(2))
+        with_t = _adjoint(sino, src, dst, Mi, b, n_row, n_col, opts, torch.empty(1, n_row, n_col, device=DEV))
+        plain = _adjoint(sino, src, dst, Mi, b, n_row, n_col, opts, None)
+        assert rel_err(with_t[0].cpu().numpy(), plain[0].cpu().numpy()) < TOL
+        if rule == 0:
+            s3, d3, M3, b3 = _embed_3d(src, dst, Mi, b)
+            ref = O.back_planesort(sino[0].cpu().numpy(), M3, b3, s3, d3, (n_row, n_col, 1))[..., 0]
+            assert rel_err(with_t[0].cpu().numpy(), ref) < TOL
+
+
 def test_scratch_adjoint_accumulates_and_is_the_transpose():
     from ct_laboratory_b200.tomography import forward_project_2d_siddon
     from ct_laboratory_b200.tomography._common import inverse
