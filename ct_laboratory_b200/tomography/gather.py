@@ -1,10 +1,19 @@
-"""Deterministic (voxel-driven gather) 3-D adjoint.
+"""Deterministic (voxel-driven gather) adjoint, 3-D and 2-D.
 
 ``back_project_3d_gather_cuda`` computes A^T y by gathering per voxel instead
 of scattering with atomics (ctlab_back_project_3d_gather): the result is
 bitwise reproducible and is the exact transpose of the forward walk with the
 crossing voxel rule.  It needs the rays grouped into flat detector panels,
 described by ``panels_from_grid``.
+
+``back_project_2d_gather_cuda`` is the 2-D one: the image is the
+one-voxel-thick volume [n_row, n_col, 1] and the rays lie in its z = 0
+plane, where the 3-D arithmetic reduces to the 2-D walk's (every term of the
+third axis is an exact zero: the z difference, its products in the affine
+and in |v|^2, and the z plane parameters, which are absent), so the gathered
+lengths are bitwise the 2-D crossing-rule segments.  Each detector line (a
+fan-beam view, a StaticCT module lit by one source) is a one-row panel
+(``panels_from_lines_2d``).
 """
 from __future__ import annotations
 
@@ -14,7 +23,8 @@ import torch
 from .. import _native as N
 from ._common import inverse, require_cuda
 
-__all__ = ["PANEL_DTYPE", "panels_from_grid", "back_project_3d_gather_cuda"]
+__all__ = ["PANEL_DTYPE", "panels_from_grid", "back_project_3d_gather_cuda", "embed_2d_geometry",
+           "panels_from_lines_2d", "back_project_2d_gather_cuda"]
 
 # numpy mirror of ctlab_panel (include/ctlab_b200.h), 96 bytes
 PANEL_DTYPE = np.dtype([("src", "<f4", 3), ("origin", "<f4", 3), ("eu", "<f4", 3), ("ev", "<f4", 3),
@@ -95,3 +105,34 @@ def back_project_3d_gather_cuda(sinogram, src, dst, M, b, n_x, n_y, n_z, panels,
                N.ptr(b), n_x, n_y, n_z, N.ptr(panels), panels.numel() // PANEL_DTYPE.itemsize, N.ptr(out),
                N.stream_of(sino))
     return out.squeeze(0) if sinogram.dim() == 1 else out
+
+
+def embed_2d_geometry(src, dst, M, b):
+    """The 2-D geometry as the z = 0 plane of a one-voxel-thick volume:
+    src3, dst3 [n_ray, 3], M3 [3, 3] (z scale 1), b3 [3]."""
+    z = torch.zeros((src.shape[0], 1), dtype=torch.float32, device=src.device)
+    src3 = torch.cat([src.to(torch.float32), z], 1).contiguous()
+    dst3 = torch.cat([dst.to(torch.float32), z], 1).contiguous()
+    M3 = torch.eye(3, dtype=torch.float32, device=M.device)
+    M3[:2, :2] = M.to(torch.float32)
+    b3 = torch.cat([b.to(torch.float32).reshape(2), torch.zeros(1, dtype=torch.float32, device=b.device)])
+    return src3, dst3, M3.contiguous(), b3.contiguous()
+
+
+def panels_from_lines_2d(src, dst, first_rays, n_cells, cell_stride=1, device=None, check=True):
+    """Panel table for 2-D rays laid out as detector lines: ``first_rays`` the
+    ray of each line's first cell, ``n_cells`` cells per line, ``cell_stride``
+    the ray-index step between cells (a fan-beam view, a StaticCT module lit
+    by one source).  Every ray of a line must share its source."""
+    z = torch.zeros((src.shape[0], 1), dtype=torch.float64, device=src.device)
+    src3 = torch.cat([src.to(torch.float64), z], 1)
+    dst3 = torch.cat([dst.to(torch.float64), z], 1)
+    return panels_from_grid(src3, dst3, first_rays, n_cells, 1, cell_stride, 0, device=device, check=check)
+
+
+def back_project_2d_gather_cuda(sinogram, geometry3, n_row, n_col, panels):
+    """Deterministic 2-D A^T y, [B, n_row, n_col] (or [n_row, n_col] for 1-D
+    y); ``geometry3`` from embed_2d_geometry."""
+    src3, dst3, M3, b3 = geometry3
+    out = back_project_3d_gather_cuda(sinogram, src3, dst3, M3, b3, n_row, n_col, 1, panels)
+    return out.reshape(*out.shape[:-1])

@@ -17,6 +17,7 @@ from typing import Optional
 import torch
 
 from .ct_projector_2d_module import CTProjector2DModule
+from .gather import panels_from_lines_2d
 
 __all__ = ["build_static_2d_geometry", "StaticCTProjector2D", "build_uniform_static_2d_geometry",
            "UniformStaticCTProjector2D"]
@@ -56,7 +57,7 @@ class StaticCTProjector2D(CTProjector2DModule):
 
     def __init__(self, n_row, n_col, M_gantry, b_gantry, source_positions, module_centers, module_orientations,
                  det_n_col, det_spacing, source_module_mask, active_sources, M, b, backend="cuda",
-                 device: Optional[torch.device] = None, precomputed_intersections=False):
+                 device: Optional[torch.device] = None, precomputed_intersections=False, deterministic_adjoint=False):
         src, dst = build_static_2d_geometry(source_positions=source_positions,
                                             module_center_positions=module_centers,
                                             module_orientations=module_orientations, det_n_col=det_n_col,
@@ -64,8 +65,13 @@ class StaticCTProjector2D(CTProjector2DModule):
                                             M_gantry=M_gantry, b_gantry=b_gantry, active_sources=active_sources)
         if device is None:
             device = torch.device("cuda" if (backend == "cuda" and torch.cuda.is_available()) else "cpu")
+        panels = None
+        if deterministic_adjoint:  # one detector line per (frame, source, module)
+            panels = panels_from_lines_2d(src, dst, list(range(0, src.shape[0], det_n_col)), det_n_col, 1,
+                                          device=device)
         super().__init__(n_row=n_row, n_col=n_col, M=M.to(device), b=b.to(device), src=src.to(device),
-                         dst=dst.to(device), backend=backend, precomputed_intersections=precomputed_intersections)
+                         dst=dst.to(device), backend=backend, precomputed_intersections=precomputed_intersections,
+                         panels=panels, deterministic_adjoint=deterministic_adjoint)
 
 
 def _ring_angles(n, device):
@@ -98,7 +104,7 @@ class UniformStaticCTProjector2D(StaticCTProjector2D):
 
     def __init__(self, n_row, n_col, M, b, n_source, source_radius, n_module, module_radius, det_n_col, det_spacing,
                  M_gantry, b_gantry, active_sources, backend="cuda", device: Optional[torch.device] = None,
-                 precomputed_intersections=False):
+                 precomputed_intersections=False, deterministic_adjoint=False):
         if device is None:
             device = torch.device("cuda" if backend == "cuda" and torch.cuda.is_available() else "cpu")
         sp, mc, mo, smm = build_uniform_static_2d_geometry(n_source=n_source, source_radius=source_radius,
@@ -111,7 +117,8 @@ class UniformStaticCTProjector2D(StaticCTProjector2D):
                          module_orientations=mo.to(device), det_n_col=det_n_col, det_spacing=det_spacing,
                          source_module_mask=smm, active_sources=active_sources.to(device), M=M.to(device),
                          b=b.to(device), backend=backend, device=device,
-                         precomputed_intersections=precomputed_intersections)
+                         precomputed_intersections=precomputed_intersections,
+                         deterministic_adjoint=deterministic_adjoint)
         self.n_source, self.source_radius = n_source, source_radius
         self.n_module, self.module_radius = n_module, module_radius
         self.det_n_col, self.det_spacing = det_n_col, det_spacing
