@@ -13,9 +13,11 @@
 //     len   = (t_out - t_in) * |v|      (0 when t_out <= t_in)
 // with every plane parameter t = (p - s) * (1/v) and the per-ray set-up
 // (t_enter, t_exit, 1/v, |v|) computed exactly as the walks in walk.cuh compute them.
-// These are bitwise the segment lengths the crossing-rule walk produces, so
-// the result is the exact transpose of that forward, accumulated in a fixed
-// order (panel, then row, then column): bitwise reproducible from run to run.
+// These are the crossing-rule walk's segment spans times |v|, bitwise the
+// lengths the atomic adjoint scatters with (the forward applies |v| to each
+// ray's sum instead, a rounding-level difference), so the result is the
+// transpose of that forward, accumulated in a fixed order (panel, then row,
+// then column): bitwise reproducible from run to run.
 //
 // Candidate cells come from projecting the voxel's eight corners (a cell is
 // a candidate when its centre lies in the bounding box of the projected

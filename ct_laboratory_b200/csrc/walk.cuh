@@ -297,7 +297,8 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
 #pragma unroll
                 for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
                 const float t1 = fminf(tm, t_exit);
-                float seg = done ? 0.f : __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+                // crossing rule: parameter spans, scaled by |v| once per ray
+                float seg = done ? 0.f : (MID ? __fmul_rn(__fsub_rn(t1, t_cur), ray_len) : __fsub_rn(t1, t_cur));
                 int v = idx;
                 if constexpr (MID) {
                     const int m = midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G);
@@ -332,7 +333,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             for (int k = 0; k < kEdge; ++k)
                 if (k < ne && el[k] > 0.f) acc = __fmaf_rn(ld_keep(vol + (unsigned)ev[k], pol), el[k], acc);
         }
-        return acc;
+        return MID ? acc : __fmul_rn(acc, ray_len);
     } else {
         if constexpr (MID) {
             float pb[NDIM], el[kEdge];
@@ -616,14 +617,14 @@ __device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, 
             for (int q = 0; q < 4; ++q) {
                 const float te = fminf(W.tnM, W.t_exit);
                 const float ts = fminf(W.tnm, te);
-                sa[q] = done ? 0.f : __fmul_rn(__fsub_rn(ts, W.t_cur), W.ray_len);
+                sa[q] = done ? 0.f : __fsub_rn(ts, W.t_cur);
                 ia[q] = W.idx;
                 if (!done && W.tnm <= te) {
                     W.idx += W.dsm;
                     W.pnm += W.psm;
                     W.tnm = plane_t(W.pnm, W.sm, W.im);
                 }
-                sb[q] = done ? 0.f : __fmul_rn(__fsub_rn(te, ts), W.ray_len);
+                sb[q] = done ? 0.f : __fsub_rn(te, ts);
                 ib[q] = W.idx;
                 W.t_cur = te;
                 done = done || !(W.tnM < W.t_exit);
@@ -645,7 +646,7 @@ __device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, 
                 if (sb[q] > 0.f) acc = __fmaf_rn(v[4 + q], sb[q], acc);
             }
         }
-        return acc;
+        return __fmul_rn(acc, W.ray_len);
     } else {
 #pragma unroll 1
         for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step<false>(W, out, y, A, G);
@@ -784,9 +785,10 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
 //     te = min(t_cell_end, t_exit)      ts = min(t_next_z, te)
 //     segment A = [t_cur, ts] in (column, k)
 //     segment B = [ts, te]    in (column, k +- 1), empty unless a z plane lies inside
-// Segments are (t1 - t0) * |v| over the same plane parameters as the per-lane
-// walk, taken in the same order, and zero-length ones are skipped as there,
-// so the results are bitwise those of traverse<3, ADJ, false>.
+// Segments are the parameter spans t1 - t0 over the same plane parameters as
+// the per-lane walk, taken in the same order, zero-length ones skipped and
+// |v| applied once per ray as there, so the results are bitwise those of
+// traverse<3, ADJ, false>.
 //
 // At most one z plane per cell: a cell spans at most the x or y plane
 // spacing in t, 1 / max(|v_x|, |v_y|), and z planes are 1 / |v_z| apart.  A
@@ -900,10 +902,10 @@ struct ZWalk {
 };
 
 // NG cells of the buffer from position q: segment A = [t_cur, ts] in
-// (column, k), segment B = [ts, te] in (column, k') after a z step.  With
-// LEN the segments are lengths (t1 - t0) * |v| (the reference's formula,
-// ct_projector_3d.cu:998); without, parameter spans t1 - t0 that the caller
-// scales by |v| itself.
+// (column, k), segment B = [ts, te] in (column, k') after a z step, as
+// parameter spans t1 - t0; the caller scales by |v| (the reference's length
+// (t1 - t0) * |v|, ct_projector_3d.cu:998) once per ray: the forward
+// multiplies its sum, the adjoint its y.
 template <int NG>
 struct CellGroup {
     float sa[NG], sb[NG];
@@ -915,21 +917,21 @@ struct CellGroup {
 // buffer is written), so a cell's end needs no clipping to the lane's exit
 // and t_cur only moves forward: two operations per cell fewer, the same
 // segments.
-template <int NG, bool LEN, bool UNI>
+template <int NG, bool UNI>
 __device__ __forceinline__ void walk_group(const XYCell* buf, int q, CellGroup<NG>& g, ZWalk& Z) {
 #pragma unroll
     for (int u = 0; u < NG; ++u) {
         const XYCell c = buf[q + u];
         const float te = UNI ? c.t : fminf(c.t, Z.t_end);
         const float ts = fminf(Z.tnz, te);
-        g.sa[u] = LEN ? __fmul_rn(__fsub_rn(ts, Z.t_cur), Z.len) : __fsub_rn(ts, Z.t_cur);
+        g.sa[u] = __fsub_rn(ts, Z.t_cur);
         g.ia[u] = (unsigned)(c.col + Z.kz);
         if (Z.tnz <= te) {  // a z plane inside the cell (or ending it)
             Z.kz += Z.dsz;
             Z.pnz += Z.psz;
             Z.tnz = plane_t(Z.pnz, Z.s2, Z.i2);
         }
-        g.sb[u] = LEN ? __fmul_rn(__fsub_rn(te, ts), Z.len) : __fsub_rn(te, ts);
+        g.sb[u] = __fsub_rn(te, ts);
         g.ib[u] = (unsigned)(c.col + Z.kz);
         Z.t_cur = UNI ? te : fmaxf(Z.t_cur, te);
     }
@@ -1192,7 +1194,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
 #pragma unroll 1
                 for (int q = 0; q < n_cells; q += kGroupAdj) {
                     CellGroup<kGroupAdj> g;
-                    walk_group<kGroupAdj, false, UNI>(buf, q, g, Z);
+                    walk_group<kGroupAdj, UNI>(buf, q, g, Z);
 #pragma unroll
                     for (int j = 0; j < NB; ++j) {
 #pragma unroll
@@ -1209,7 +1211,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
 #pragma unroll 1
                 for (int q = 0; q < n_cells; q += kGF) {
                     CellGroup<kGF> g;
-                    walk_group<kGF, true, UNI>(buf, q, g, Z);
+                    walk_group<kGF, UNI>(buf, q, g, Z);
                     float v[NB][2 * kGF];
 #pragma unroll
                     for (int j = 0; j < NB; ++j) gather_group<kGF>(vol[j], g, v[j], pol);
@@ -1242,7 +1244,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
         if (r >= 0) {
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, acc[j]);
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(acc[j], Z.len));
         }
     }
 }
