@@ -87,6 +87,7 @@ _SIGS = {
     "ctlab_back_project_2d_siddon_ws": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _I, _TP, _P, _P],
     "ctlab_invert_matrix": [_P, _I, _P, _P, _P],
     "ctlab_back_project_3d_gather": [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I64, _P, _P],
+    "ctlab_back_project_3d_gather_ws": [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I64, _P, _P, _P],
     "ctlab_batch_plan": [_SP, _I32, _I32, _P, _I64, _BP, _P],
     "ctlab_forward_project_batched": [_BP, _I32, _P],
     "ctlab_back_project_batched": [_BP, _I, _I32, _P],

@@ -12,7 +12,8 @@
 //     t_out = min(t_exit,  ahead-plane parameters of the voxel)
 //     len   = (t_out - t_in) * |v|      (0 when t_out <= t_in)
 // with every plane parameter t = (p - s) * (1/v) and the per-ray set-up
-// (t_enter, t_exit, 1/v, |v|) computed exactly as the walks in walk.cuh compute them.
+// (s, 1/v, |v|) computed exactly as the walks in walk.cuh compute them (t_enter
+// and t_exit need not be: see RaySetup).
 // These are the crossing-rule walk's segment spans times |v|, bitwise the
 // lengths the atomic adjoint scatters with (the forward applies |v| to each
 // ray's sum instead, a rounding-level difference), so the result is the
@@ -23,6 +24,9 @@
 // a candidate when its centre lies in the bounding box of the projected
 // corners, widened by a small margin); the exact length test then discards
 // rays that miss, so the margin only costs time.
+#include <algorithm>
+#include <cstdint>
+
 #include "common.cuh"
 
 namespace ctlab {
@@ -35,15 +39,22 @@ struct PanelDev {
     int n_u, n_v;
 };
 
-// Same set-up as lane_setup / traverse in walk.cuh.
+// The per-ray values of lane_setup in walk.cuh that a voxel's length needs,
+// computed with the same arithmetic.  The ray's entry and exit parameters are
+// not: along every crossed axis the voxel's own behind / ahead plane lies
+// inside the grid's, and t = (p - s) * (1/v) is monotone in p under
+// round-to-nearest, so max(t_enter, voxel behind-planes) equals
+// max(0, voxel behind-planes) bitwise, and likewise for the exit with 1.  A
+// ray that misses the grid gets an empty interval for every voxel the same
+// way.
 struct RaySetup {
-    float s[3], inv[3], ray_len, t_enter, t_exit;
+    float s[3], inv[3], ray_len;
     int fixed[3];  // index along an axis the ray does not cross, else -1
     bool live;
 };
 
 __device__ __forceinline__ RaySetup ray_setup(const float* __restrict__ src, const float* __restrict__ dst,
-                                              int64_t r, const Affine3& A, const int* n) {
+                                              int64_t r, const Affine3& A) {
     RaySetup R;
     float sw[3], dw[3], vw[3], d[3];
 #pragma unroll
@@ -56,33 +67,24 @@ __device__ __forceinline__ RaySetup ray_setup(const float* __restrict__ src, con
     R.live = R.ray_len >= 1e-12f;
     world_to_index3(A, sw[0], sw[1], sw[2], R.s[0], R.s[1], R.s[2]);
     world_to_index3(A, dw[0], dw[1], dw[2], d[0], d[1], d[2]);
-    R.t_enter = 0.f;
-    R.t_exit = 1.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float va = __fsub_rn(d[a], R.s[a]);
-        const float nf = (float)n[a];
         R.live = R.live && isfinite(R.s[a]) && isfinite(va);
         if (fabsf(va) > 1e-12f) {
             R.inv[a] = __frcp_rn(va);
             R.fixed[a] = -1;
-            const float lo = va > 0.f ? -0.5f : nf - 0.5f;
-            const float hi = va > 0.f ? nf - 0.5f : -0.5f;
-            R.t_enter = fmaxf(R.t_enter, plane_t(lo, R.s[a], R.inv[a]));
-            R.t_exit = fminf(R.t_exit, plane_t(hi, R.s[a], R.inv[a]));
         } else {
             R.inv[a] = 0.f;
             R.fixed[a] = __float2int_rn(R.s[a]);
-            R.live = R.live && R.fixed[a] >= 0 && R.fixed[a] < n[a];
         }
     }
-    R.live = R.live && (R.t_enter < R.t_exit);
     return R;
 }
 
 // Intersection length of a set-up ray with voxel (i, j, k).
 __device__ __forceinline__ float voxel_len(const RaySetup& R, const int* ijk) {
-    float t_in = R.t_enter, t_out = R.t_exit;
+    float t_in = 0.f, t_out = 1.f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         if (R.inv[a] != 0.f) {
@@ -98,105 +100,216 @@ __device__ __forceinline__ float voxel_len(const RaySetup& R, const int* ijk) {
     return t_out > t_in ? __fmul_rn(__fsub_rn(t_out, t_in), R.ray_len) : 0.f;
 }
 
+// The ray table: per ray s[3] and |v| (0 for a ray the walk skips), then
+// 1/v[3] (0 along an axis the ray does not cross, where s rounds to the
+// fixed index), 32 bytes, read as two float4.
+struct __align__(16) RayRow {
+    float s[3], ray_len;
+    float inv[3], pad;
+};
+static_assert(sizeof(RayRow) == 32, "ray table row");
+
+__global__ void __launch_bounds__(256) gather_ray_table_kernel(const float* __restrict__ src,
+                                                               const float* __restrict__ dst, int64_t n_ray,
+                                                               const float* __restrict__ M_inv,
+                                                               const float* __restrict__ bvec, RayRow* __restrict__ tab) {
+    const Affine3 A = load_affine3(M_inv, bvec);
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_ray; r += (int64_t)gridDim.x * blockDim.x) {
+        const RaySetup R = ray_setup(src, dst, r, A);
+        RayRow row;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            row.s[a] = R.s[a];
+            row.inv[a] = R.inv[a];
+        }
+        row.ray_len = R.live ? R.ray_len : 0.f;
+        row.pad = 0.f;
+        tab[r] = row;
+    }
+}
+
+__device__ __forceinline__ float voxel_len_row(const float4 a, const float4 b, const int* ijk) {
+    const float s[3] = {a.x, a.y, a.z}, inv[3] = {b.x, b.y, b.z};
+    float t_in = 0.f, t_out = 1.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (inv[k] != 0.f) {
+            const float p0 = (float)ijk[k] - 0.5f, p1 = (float)ijk[k] + 0.5f;
+            const float ta = plane_t(p0, s[k], inv[k]), tb = plane_t(p1, s[k], inv[k]);
+            const bool pos = inv[k] > 0.f;
+            t_in = fmaxf(t_in, pos ? ta : tb);
+            t_out = fminf(t_out, pos ? tb : ta);
+        } else if (__float2int_rn(s[k]) != ijk[k]) {
+            return 0.f;
+        }
+    }
+    return t_out > t_in ? __fmul_rn(__fsub_rn(t_out, t_in), a.w) : 0.f;
+}
+
+// What the corner projection needs of a panel, derived once per launch
+// block: with q = X - S for a point X,
+//     u(X) = base_u + lam * (q . eu),  v(X) = base_v + lam * (q . ev),
+//     lam  = nd / (q . n),  nd = n . (O - S),
+// and q . e over the eight corners X = centre +- h0 +- h1 +- h2 (h_a the
+// half voxel edges in world space) is (centre - S) . e +- h0.e +- h1.e +- h2.e.
+struct PanelProj {
+    float src[3], n[3], eu[3], ev[3];
+    float nd, base_u, base_v, pad;
+    float hn[3], hu[3], hv[3];
+    int n_u, n_v;
+    long long first_ray, u_stride, v_stride;
+};
+
+constexpr int kPanelChunk = 64;
+
+__device__ __forceinline__ void panel_proj(const PanelDev& P, const float* __restrict__ M, PanelProj& Q) {
+    float so[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        Q.src[r] = P.src[r];
+        Q.n[r] = P.n[r];
+        Q.eu[r] = P.eu[r];
+        Q.ev[r] = P.ev[r];
+        so[r] = P.src[r] - P.origin[r];
+    }
+    Q.nd = -(so[0] * P.n[0] + so[1] * P.n[1] + so[2] * P.n[2]);
+    Q.base_u = so[0] * P.eu[0] + so[1] * P.eu[1] + so[2] * P.eu[2];
+    Q.base_v = so[0] * P.ev[0] + so[1] * P.ev[1] + so[2] * P.ev[2];
+    Q.pad = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float h[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) h[r] = 0.5f * __ldg(M + 3 * r + a);
+        Q.hn[a] = h[0] * P.n[0] + h[1] * P.n[1] + h[2] * P.n[2];
+        Q.hu[a] = h[0] * P.eu[0] + h[1] * P.eu[1] + h[2] * P.eu[2];
+        Q.hv[a] = h[0] * P.ev[0] + h[1] * P.ev[1] + h[2] * P.ev[2];
+    }
+    Q.n_u = P.n_u;
+    Q.n_v = P.n_v;
+    Q.first_ray = P.first_ray;
+    Q.u_stride = P.u_stride;
+    Q.v_stride = P.v_stride;
+}
+
+// The eight corner values x0 +- h0 +- h1 +- h2.
+__device__ __forceinline__ void corner_values(float x0, const float* h, float* out) {
+    const float a0 = x0 - h[0], a1 = x0 + h[0];
+    const float b0 = a0 - h[1], b1 = a1 - h[1], b2 = a0 + h[1], b3 = a1 + h[1];
+    out[0] = b0 - h[2];
+    out[1] = b1 - h[2];
+    out[2] = b2 - h[2];
+    out[3] = b3 - h[2];
+    out[4] = b0 + h[2];
+    out[5] = b1 + h[2];
+    out[6] = b2 + h[2];
+    out[7] = b3 + h[2];
+}
+
+// One thread per voxel (z fastest, so a warp holds 32 neighbours along z,
+// whose footprints share detector columns).  The panels are taken in chunks
+// staged in shared memory; every thread of the block takes part in staging,
+// voxels past the grid included.
+// TAB: the rays' set-up comes from the ray table (tab), else it is
+// recomputed for every candidate; the lengths are the same bitwise.
+template <bool TAB>
 __global__ void __launch_bounds__(256) gather3d_kernel(const float* __restrict__ sino, float* __restrict__ out,
                                                        const float* __restrict__ src, const float* __restrict__ dst,
                                                        int64_t n_ray, const float* __restrict__ M_inv,
                                                        const float* __restrict__ bvec, const float* __restrict__ M,
                                                        int nx, int ny, int nz, const PanelDev* __restrict__ panels,
-                                                       int n_panel, float margin) {
+                                                       int n_panel, float margin, const float4* __restrict__ tab) {
+    __shared__ PanelProj sp[kPanelChunk];
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nvox = (int64_t)nx * ny * nz;
-    if (v >= nvox) return;
+    const bool active = v < nvox;
     const int64_t bi = blockIdx.y;
-    const int n[3] = {nx, ny, nz};
-    const int ijk[3] = {(int)(v / ((int64_t)ny * nz)), (int)((v / nz) % ny), (int)(v % nz)};
+    const int64_t vc = active ? v : 0;
+    const int ijk[3] = {(int)(vc / ((int64_t)ny * nz)), (int)((vc / nz) % ny), (int)(vc % nz)};
     const Affine3 A = load_affine3(M_inv, bvec);
-    // voxel centre and half-edge vectors in world space: x = M (ijk) + b
-    float c[3], h[3][3];
+    // voxel centre in world space: x = M (ijk) + b
+    float c[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         c[r] = __ldg(bvec + r);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float m = __ldg(M + 3 * r + a);
-            c[r] = __fmaf_rn(m, (float)ijk[a], c[r]);
-            h[a][r] = 0.5f * m;
-        }
+        for (int a = 0; a < 3; ++a) c[r] = __fmaf_rn(__ldg(M + 3 * r + a), (float)ijk[a], c[r]);
     }
     const float* y = sino + bi * n_ray;
     float acc = 0.f;
-    for (int p = 0; p < n_panel; ++p) {
-        const PanelDev& P = panels[p];
-        // project the eight corners: u = ((S - O) + lam (X - S)) . eu with
-        // lam = n.(O - S) / n.(X - S)
-        float so[3], q0[3];
+    for (int p0 = 0; p0 < n_panel; p0 += kPanelChunk) {
+        const int np = min(kPanelChunk, n_panel - p0);
+        __syncthreads();  // the previous chunk is no longer read
+        if ((int)threadIdx.x < np) panel_proj(panels[p0 + threadIdx.x], M, sp[threadIdx.x]);
+        __syncthreads();
+        if (!active) continue;
+#pragma unroll 1
+        for (int p = 0; p < np; ++p) {
+            const PanelProj& Q = sp[p];
+            const float q0[3] = {c[0] - Q.src[0], c[1] - Q.src[1], c[2] - Q.src[2]};
+            float cn[8], cu[8], cv[8];
+            corner_values(q0[0] * Q.n[0] + q0[1] * Q.n[1] + q0[2] * Q.n[2], Q.hn, cn);
+            corner_values(q0[0] * Q.eu[0] + q0[1] * Q.eu[1] + q0[2] * Q.eu[2], Q.hu, cu);
+            corner_values(q0[0] * Q.ev[0] + q0[1] * Q.ev[1] + q0[2] * Q.ev[2], Q.hv, cv);
+            float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+            bool behind = false;
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            so[r] = P.src[r] - P.origin[r];
-            q0[r] = c[r] - P.src[r];
-        }
-        const float nd = -(so[0] * P.n[0] + so[1] * P.n[1] + so[2] * P.n[2]);
-        const float base_u = so[0] * P.eu[0] + so[1] * P.eu[1] + so[2] * P.eu[2];
-        const float base_v = so[0] * P.ev[0] + so[1] * P.ev[1] + so[2] * P.ev[2];
-        float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
-        bool behind = false;
-#pragma unroll
-        for (int corner = 0; corner < 8; ++corner) {
-            float q[3];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                q[r] = q0[r];
-#pragma unroll
-                for (int a = 0; a < 3; ++a) q[r] += ((corner >> a) & 1 ? h[a][r] : -h[a][r]);
+            for (int k = 0; k < 8; ++k) {
+                // a corner at or behind the source plane: the footprint is unbounded
+                behind = behind || !(cn[k] * Q.nd > 0.f);
+                const float lam = __fdividef(Q.nd, cn[k]);
+                const float u = __fmaf_rn(lam, cu[k], Q.base_u);
+                const float w = __fmaf_rn(lam, cv[k], Q.base_v);
+                umin = fminf(umin, u);
+                umax = fmaxf(umax, u);
+                vmin = fminf(vmin, w);
+                vmax = fmaxf(vmax, w);
             }
-            const float qn = q[0] * P.n[0] + q[1] * P.n[1] + q[2] * P.n[2];
-            // a corner at or behind the source plane: the footprint is unbounded
-            behind = behind || !(qn * nd > 0.f);
-            const float lam = nd / qn;
-            const float u = base_u + lam * (q[0] * P.eu[0] + q[1] * P.eu[1] + q[2] * P.eu[2]);
-            const float w = base_v + lam * (q[0] * P.ev[0] + q[1] * P.ev[1] + q[2] * P.ev[2]);
-            umin = fminf(umin, u);
-            umax = fmaxf(umax, u);
-            vmin = fminf(vmin, w);
-            vmax = fmaxf(vmax, w);
-        }
-        int u0, u1, v0, v1;
-        if (behind) {
-            u0 = 0;
-            u1 = P.n_u - 1;
-            v0 = 0;
-            v1 = P.n_v - 1;
-        } else {
-            u0 = max(0, (int)ceilf(umin - margin));
-            u1 = min(P.n_u - 1, (int)floorf(umax + margin));
-            v0 = max(0, (int)ceilf(vmin - margin));
-            v1 = min(P.n_v - 1, (int)floorf(vmax + margin));
-        }
-        for (int jv = v0; jv <= v1; ++jv) {
-            for (int ju = u0; ju <= u1; ++ju) {
-                const int64_t r = P.first_ray + (int64_t)jv * P.v_stride + (int64_t)ju * P.u_stride;
-                const float yr = __ldg(y + r);
-                if (yr == 0.f) continue;
-                const RaySetup R = ray_setup(src, dst, r, A, n);
-                if (!R.live) continue;
-                const float len = voxel_len(R, ijk);
-                if (len > 0.f) acc = __fmaf_rn(yr, len, acc);
+            int u0, u1, v0, v1;
+            if (behind) {
+                u0 = 0;
+                u1 = Q.n_u - 1;
+                v0 = 0;
+                v1 = Q.n_v - 1;
+            } else {
+                u0 = max(0, (int)ceilf(umin - margin));
+                u1 = min(Q.n_u - 1, (int)floorf(umax + margin));
+                v0 = max(0, (int)ceilf(vmin - margin));
+                v1 = min(Q.n_v - 1, (int)floorf(vmax + margin));
+            }
+            for (int jv = v0; jv <= v1; ++jv) {
+                for (int ju = u0; ju <= u1; ++ju) {
+                    const int64_t r = Q.first_ray + (int64_t)jv * Q.v_stride + (int64_t)ju * Q.u_stride;
+                    const float yr = __ldg(y + r);
+                    if (yr == 0.f) continue;
+                    float len;
+                    if constexpr (TAB) {
+                        const float4 ra = __ldg(tab + 2 * r);
+                        if (!(ra.w > 0.f)) continue;
+                        len = voxel_len_row(ra, __ldg(tab + 2 * r + 1), ijk);
+                    } else {
+                        const RaySetup R = ray_setup(src, dst, r, A);
+                        if (!R.live) continue;
+                        len = voxel_len(R, ijk);
+                    }
+                    if (len > 0.f) acc = __fmaf_rn(yr, len, acc);
+                }
             }
         }
     }
-    out[bi * nvox + v] = acc;
+    if (active) out[bi * nvox + v] = acc;
 }
 
 }  // namespace ctlab
 
 using namespace ctlab;
 
-extern "C" int ctlab_back_project_3d_gather(const float* sino, int64_t batch, int64_t n_ray, const float* src,
-                                            const float* dst, const float* M, const float* M_inv, const float* b,
-                                            int64_t n_x, int64_t n_y, int64_t n_z, const ctlab_panel* panels,
-                                            int64_t n_panel, float* out, void* stream) {
+namespace {
+
+int gather_entry(const char* what, const float* sino, int64_t batch, int64_t n_ray, const float* src, const float* dst,
+                 const float* M, const float* M_inv, const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
+                 const ctlab_panel* panels, int64_t n_panel, float* out, void* ray_table, void* stream) {
     clear_error();
-    const char* what = "back_project_3d_gather";
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535]", what);
     CTLAB_REQUIRE(n_ray >= 0 && n_panel >= 0 && n_panel < (1LL << 31), "%s: bad n_ray/n_panel", what);
     CTLAB_REQUIRE(n_x >= 1 && n_y >= 1 && n_z >= 1 && n_x <= (1 << 22) && n_y <= (1 << 22) && n_z <= (1 << 22),
@@ -205,10 +318,39 @@ extern "C" int ctlab_back_project_3d_gather(const float* sino, int64_t batch, in
     CTLAB_REQUIRE(nvox < (1LL << 31), "%s: volume too large", what);
     CTLAB_REQUIRE(out && M && M_inv && b && (n_panel == 0 || panels) && (n_ray == 0 || (sino && src && dst)),
                   "%s: null pointer", what);
+    CTLAB_REQUIRE(((uintptr_t)ray_table & 15) == 0, "%s: ray_table must be 16-byte aligned", what);
     const int64_t blocks = (nvox + 255) / 256;
     static_assert(sizeof(ctlab_panel) == sizeof(PanelDev), "panel layout");
-    gather3d_kernel<<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, as_stream(stream)>>>(
-        sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z,
-        reinterpret_cast<const PanelDev*>(panels), (int)n_panel, 0.05f);
+    cudaStream_t st = as_stream(stream);
+    const PanelDev* pd = reinterpret_cast<const PanelDev*>(panels);
+    if (ray_table && n_ray > 0) {
+        const int64_t tb = std::min<int64_t>((n_ray + 255) / 256, 148 * 64);
+        gather_ray_table_kernel<<<(unsigned)tb, 256, 0, st>>>(src, dst, n_ray, M_inv, b,
+                                                              static_cast<RayRow*>(ray_table));
+        gather3d_kernel<true><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
+            sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f,
+            static_cast<const float4*>(ray_table));
+    } else {
+        gather3d_kernel<false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
+            sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, nullptr);
+    }
     return launch_status(what);
+}
+
+}  // namespace
+
+extern "C" int ctlab_back_project_3d_gather(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                            const float* dst, const float* M, const float* M_inv, const float* b,
+                                            int64_t n_x, int64_t n_y, int64_t n_z, const ctlab_panel* panels,
+                                            int64_t n_panel, float* out, void* stream) {
+    return gather_entry("back_project_3d_gather", sino, batch, n_ray, src, dst, M, M_inv, b, n_x, n_y, n_z, panels,
+                        n_panel, out, nullptr, stream);
+}
+
+extern "C" int ctlab_back_project_3d_gather_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                               const float* dst, const float* M, const float* M_inv, const float* b,
+                                               int64_t n_x, int64_t n_y, int64_t n_z, const ctlab_panel* panels,
+                                               int64_t n_panel, float* out, void* ray_table, void* stream) {
+    return gather_entry("back_project_3d_gather_ws", sino, batch, n_ray, src, dst, M, M_inv, b, n_x, n_y, n_z,
+                        panels, n_panel, out, ray_table, stream);
 }

@@ -100,10 +100,12 @@ def back_project_3d_gather_cuda(sinogram, src, dst, M, b, n_x, n_y, n_z, panels,
     if panels.dtype != torch.uint8 or panels.numel() % PANEL_DTYPE.itemsize:
         raise RuntimeError("panels must be the uint8 table from panels_from_grid")
     out = torch.empty((batch, n_x, n_y, n_z), device=sino.device, dtype=torch.float32)
+    # the ray table: each ray's set-up once, 32 bytes per ray
+    table = torch.empty((max(int(n_ray), 1), 8), device=sino.device, dtype=torch.float32)
     with torch.cuda.device(sino.device):
-        N.call("ctlab_back_project_3d_gather", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst), N.ptr(M), N.ptr(Mi),
-               N.ptr(b), n_x, n_y, n_z, N.ptr(panels), panels.numel() // PANEL_DTYPE.itemsize, N.ptr(out),
-               N.stream_of(sino))
+        N.call("ctlab_back_project_3d_gather_ws", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst), N.ptr(M),
+               N.ptr(Mi), N.ptr(b), n_x, n_y, n_z, N.ptr(panels), panels.numel() // PANEL_DTYPE.itemsize, N.ptr(out),
+               N.ptr(table), N.stream_of(sino))
     return out.squeeze(0) if sinogram.dim() == 1 else out
 
 

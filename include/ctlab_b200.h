@@ -147,8 +147,9 @@ typedef struct ctlab_panel {
 
 /* Deterministic adjoint by gathering: every voxel sums y[b, r] * len(r, voxel)
  * over the rays of each panel that can reach it, in a fixed order, with
- * len evaluated by the arithmetic of the crossing-rule forward walk.  It is
- * bitwise reproducible, and is the exact transpose of
+ * len evaluated by the arithmetic of the crossing-rule walk (bitwise the
+ * lengths the atomic crossing-rule adjoint scatters).  It is bitwise
+ * reproducible, and is the transpose of
  * ctlab_forward_project_3d_on_the_fly_ex with CTLAB_VOXEL_CROSSING.  No
  * counterpart in the reference (its adjoints all scatter with atomicAdd,
  * src/ct_projector_3d.cu:267, :374, :1005).  `M` is the voxel-index -> world
@@ -156,6 +157,16 @@ typedef struct ctlab_panel {
 int ctlab_back_project_3d_gather(const float* sino, int64_t batch, int64_t n_ray, const float* src, const float* dst,
                                  const float* M, const float* M_inv, const float* b, int64_t n_x, int64_t n_y,
                                  int64_t n_z, const ctlab_panel* panels, int64_t n_panel, float* out, void* stream);
+
+/* ctlab_back_project_3d_gather with a caller-provided device workspace
+ * `ray_table` of 32 * n_ray bytes, 16-byte aligned (NULL: as
+ * ctlab_back_project_3d_gather): each ray's set-up (its source in index
+ * space, 1/v and |v|) is computed into it once instead of once per voxel that
+ * the ray can reach.  The result is bitwise the same. */
+int ctlab_back_project_3d_gather_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                    const float* dst, const float* M, const float* M_inv, const float* b, int64_t n_x,
+                                    int64_t n_y, int64_t n_z, const ctlab_panel* panels, int64_t n_panel, float* out,
+                                    void* ray_table, void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* 3-D, precomputed intersections                                          */

@@ -283,6 +283,12 @@ def test_deterministic_gather_adjoint():
     g1 = back_project_3d_gather_cuda(T(y), src, dst, M, b, *dims, panels)
     g2 = back_project_3d_gather_cuda(T(y), src, dst, M, b, *dims, panels)
     assert torch.equal(g1, g2)
+    # the entry without a ray table (each candidate's set-up recomputed): bitwise the same
+    from ct_laboratory_b200.tomography._common import inverse
+    yt, g0 = T(y), torch.empty_like(g1)
+    N.call("ctlab_back_project_3d_gather", N.ptr(yt), 2, yt.shape[1], N.ptr(src), N.ptr(dst), N.ptr(M),
+           N.ptr(inverse(M)), N.ptr(b), *dims, N.ptr(panels), n_view, N.ptr(g0), N.stream_of(yt))
+    assert torch.equal(g0, g1)
     opts = N.tiling(n_view, nv, nu, nv * nu, nu, 1, voxel_rule=N.VOXEL_CROSSING)
     at = C.back_project_3d_on_the_fly_cuda(T(y), src, dst, Mi, b, *dims, tiling=opts)
     assert rel_err(g1.cpu().numpy(), at.cpu().numpy()) < 1e-6
