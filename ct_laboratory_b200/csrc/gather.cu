@@ -102,17 +102,19 @@ __device__ __forceinline__ float voxel_len(const RaySetup& R, const int* ijk) {
 
 // The ray table: per ray s[3] and |v| (0 for a ray the walk skips), then
 // 1/v[3] (0 along an axis the ray does not cross, where s rounds to the
-// fixed index), 32 bytes, read as two float4.
+// fixed index) and y (for a single sinogram; 0 for a skipped ray), 32 bytes,
+// one sector, read as two float4.
 struct __align__(16) RayRow {
     float s[3], ray_len;
-    float inv[3], pad;
+    float inv[3], y;
 };
 static_assert(sizeof(RayRow) == 32, "ray table row");
 
 __global__ void __launch_bounds__(256) gather_ray_table_kernel(const float* __restrict__ src,
                                                                const float* __restrict__ dst, int64_t n_ray,
                                                                const float* __restrict__ M_inv,
-                                                               const float* __restrict__ bvec, RayRow* __restrict__ tab) {
+                                                               const float* __restrict__ bvec,
+                                                               const float* __restrict__ y, RayRow* __restrict__ tab) {
     const Affine3 A = load_affine3(M_inv, bvec);
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n_ray; r += (int64_t)gridDim.x * blockDim.x) {
         const RaySetup R = ray_setup(src, dst, r, A);
@@ -123,7 +125,7 @@ __global__ void __launch_bounds__(256) gather_ray_table_kernel(const float* __re
             row.inv[a] = R.inv[a];
         }
         row.ray_len = R.live ? R.ray_len : 0.f;
-        row.pad = 0.f;
+        row.y = (y != nullptr && R.live) ? __ldg(y + r) : 0.f;
         tab[r] = row;
     }
 }
@@ -152,12 +154,16 @@ __device__ __forceinline__ float voxel_len_row(const float4 a, const float4 b, c
 //     lam  = nd / (q . n),  nd = n . (O - S),
 // and q . e over the eight corners X = centre +- h0 +- h1 +- h2 (h_a the
 // half voxel edges in world space) is (centre - S) . e +- h0.e +- h1.e +- h2.e.
-struct PanelProj {
-    float src[3], n[3], eu[3], ev[3];
-    float nd, base_u, base_v, pad;
-    float hn[3], hu[3], hv[3];
-    int n_u, n_v;
-    long long first_ray, u_stride, v_stride;
+// Packed in 16-byte fields: a warp reads each with one broadcast.
+struct __align__(16) PanelProj {
+    float4 s_nd;   // S, nd
+    float4 n_bu;   // n, base_u
+    float4 eu_bv;  // eu, base_v
+    float4 ev;     // ev, 0
+    float4 hn, hu, hv;
+    int4 dims;            // n_u, n_v
+    longlong2 first_us;   // first_ray, u_stride
+    longlong2 vs;         // v_stride
 };
 
 constexpr int kPanelChunk = 64;
@@ -165,60 +171,65 @@ constexpr int kPanelChunk = 64;
 __device__ __forceinline__ void panel_proj(const PanelDev& P, const float* __restrict__ M, PanelProj& Q) {
     float so[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        Q.src[r] = P.src[r];
-        Q.n[r] = P.n[r];
-        Q.eu[r] = P.eu[r];
-        Q.ev[r] = P.ev[r];
-        so[r] = P.src[r] - P.origin[r];
-    }
-    Q.nd = -(so[0] * P.n[0] + so[1] * P.n[1] + so[2] * P.n[2]);
-    Q.base_u = so[0] * P.eu[0] + so[1] * P.eu[1] + so[2] * P.eu[2];
-    Q.base_v = so[0] * P.ev[0] + so[1] * P.ev[1] + so[2] * P.ev[2];
-    Q.pad = 0.f;
+    for (int r = 0; r < 3; ++r) so[r] = P.src[r] - P.origin[r];
+    const float nd = -(so[0] * P.n[0] + so[1] * P.n[1] + so[2] * P.n[2]);
+    const float bu = so[0] * P.eu[0] + so[1] * P.eu[1] + so[2] * P.eu[2];
+    const float bv = so[0] * P.ev[0] + so[1] * P.ev[1] + so[2] * P.ev[2];
+    Q.s_nd = make_float4(P.src[0], P.src[1], P.src[2], nd);
+    Q.n_bu = make_float4(P.n[0], P.n[1], P.n[2], bu);
+    Q.eu_bv = make_float4(P.eu[0], P.eu[1], P.eu[2], bv);
+    Q.ev = make_float4(P.ev[0], P.ev[1], P.ev[2], 0.f);
+    float hn[3], hu[3], hv[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float h[3];
 #pragma unroll
         for (int r = 0; r < 3; ++r) h[r] = 0.5f * __ldg(M + 3 * r + a);
-        Q.hn[a] = h[0] * P.n[0] + h[1] * P.n[1] + h[2] * P.n[2];
-        Q.hu[a] = h[0] * P.eu[0] + h[1] * P.eu[1] + h[2] * P.eu[2];
-        Q.hv[a] = h[0] * P.ev[0] + h[1] * P.ev[1] + h[2] * P.ev[2];
+        hn[a] = h[0] * P.n[0] + h[1] * P.n[1] + h[2] * P.n[2];
+        hu[a] = h[0] * P.eu[0] + h[1] * P.eu[1] + h[2] * P.eu[2];
+        hv[a] = h[0] * P.ev[0] + h[1] * P.ev[1] + h[2] * P.ev[2];
     }
-    Q.n_u = P.n_u;
-    Q.n_v = P.n_v;
-    Q.first_ray = P.first_ray;
-    Q.u_stride = P.u_stride;
-    Q.v_stride = P.v_stride;
+    Q.hn = make_float4(hn[0], hn[1], hn[2], 0.f);
+    Q.hu = make_float4(hu[0], hu[1], hu[2], 0.f);
+    Q.hv = make_float4(hv[0], hv[1], hv[2], 0.f);
+    Q.dims = make_int4(P.n_u, P.n_v, 0, 0);
+    Q.first_us = make_longlong2(P.first_ray, P.u_stride);
+    Q.vs = make_longlong2(P.v_stride, 0);
 }
 
 // The eight corner values x0 +- h0 +- h1 +- h2.
-__device__ __forceinline__ void corner_values(float x0, const float* h, float* out) {
-    const float a0 = x0 - h[0], a1 = x0 + h[0];
-    const float b0 = a0 - h[1], b1 = a1 - h[1], b2 = a0 + h[1], b3 = a1 + h[1];
-    out[0] = b0 - h[2];
-    out[1] = b1 - h[2];
-    out[2] = b2 - h[2];
-    out[3] = b3 - h[2];
-    out[4] = b0 + h[2];
-    out[5] = b1 + h[2];
-    out[6] = b2 + h[2];
-    out[7] = b3 + h[2];
+__device__ __forceinline__ void corner_values(float x0, const float4 h, float* out) {
+    const float a0 = x0 - h.x, a1 = x0 + h.x;
+    const float b0 = a0 - h.y, b1 = a1 - h.y, b2 = a0 + h.y, b3 = a1 + h.y;
+    out[0] = b0 - h.z;
+    out[1] = b1 - h.z;
+    out[2] = b2 - h.z;
+    out[3] = b3 - h.z;
+    out[4] = b0 + h.z;
+    out[5] = b1 + h.z;
+    out[6] = b2 + h.z;
+    out[7] = b3 + h.z;
 }
 
 // One thread per voxel (z fastest, so a warp holds 32 neighbours along z,
 // whose footprints share detector columns).  The panels are taken in chunks
 // staged in shared memory; every thread of the block takes part in staging,
-// voxels past the grid included.
+// voxels past the grid included (with no candidates).
 // TAB: the rays' set-up comes from the ray table (tab), else it is
-// recomputed for every candidate; the lengths are the same bitwise.
-template <bool TAB>
-__global__ void __launch_bounds__(256) gather3d_kernel(const float* __restrict__ sino, float* __restrict__ out,
+// recomputed for every candidate; the lengths are the same bitwise.  YT: y
+// comes from the table too (one sinogram), so a candidate is one 32-byte
+// sector.  (Staging a warp's candidate rows in shared memory first, read
+// coalesced along detector rows, measured slower: 97.8 against 82.8 ms on
+// the cone256 scan; each row is read by every warp whose voxels it crosses
+// either way.)
+template <bool TAB, bool YT>
+__global__ void __launch_bounds__(256, TAB ? 4 : 3) gather3d_kernel(const float* __restrict__ sino, float* __restrict__ out,
                                                        const float* __restrict__ src, const float* __restrict__ dst,
                                                        int64_t n_ray, const float* __restrict__ M_inv,
                                                        const float* __restrict__ bvec, const float* __restrict__ M,
                                                        int nx, int ny, int nz, const PanelDev* __restrict__ panels,
                                                        int n_panel, float margin, const float4* __restrict__ tab) {
+    static_assert(TAB || !YT, "y in the table needs the table");
     __shared__ PanelProj sp[kPanelChunk];
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nvox = (int64_t)nx * ny * nz;
@@ -227,6 +238,7 @@ __global__ void __launch_bounds__(256) gather3d_kernel(const float* __restrict__
     const int64_t vc = active ? v : 0;
     const int ijk[3] = {(int)(vc / ((int64_t)ny * nz)), (int)((vc / nz) % ny), (int)(vc % nz)};
     const Affine3 A = load_affine3(M_inv, bvec);
+    (void)A;
     // voxel centre in world space: x = M (ijk) + b
     float c[3];
 #pragma unroll
@@ -242,52 +254,66 @@ __global__ void __launch_bounds__(256) gather3d_kernel(const float* __restrict__
         __syncthreads();  // the previous chunk is no longer read
         if ((int)threadIdx.x < np) panel_proj(panels[p0 + threadIdx.x], M, sp[threadIdx.x]);
         __syncthreads();
-        if (!active) continue;
 #pragma unroll 1
         for (int p = 0; p < np; ++p) {
-            const PanelProj& Q = sp[p];
-            const float q0[3] = {c[0] - Q.src[0], c[1] - Q.src[1], c[2] - Q.src[2]};
+            const float4 s_nd = sp[p].s_nd, n_bu = sp[p].n_bu, eu_bv = sp[p].eu_bv, ev = sp[p].ev;
+            const float q0[3] = {c[0] - s_nd.x, c[1] - s_nd.y, c[2] - s_nd.z};
             float cn[8], cu[8], cv[8];
-            corner_values(q0[0] * Q.n[0] + q0[1] * Q.n[1] + q0[2] * Q.n[2], Q.hn, cn);
-            corner_values(q0[0] * Q.eu[0] + q0[1] * Q.eu[1] + q0[2] * Q.eu[2], Q.hu, cu);
-            corner_values(q0[0] * Q.ev[0] + q0[1] * Q.ev[1] + q0[2] * Q.ev[2], Q.hv, cv);
+            corner_values(q0[0] * n_bu.x + q0[1] * n_bu.y + q0[2] * n_bu.z, sp[p].hn, cn);
+            corner_values(q0[0] * eu_bv.x + q0[1] * eu_bv.y + q0[2] * eu_bv.z, sp[p].hu, cu);
+            corner_values(q0[0] * ev.x + q0[1] * ev.y + q0[2] * ev.z, sp[p].hv, cv);
             float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
             bool behind = false;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 // a corner at or behind the source plane: the footprint is unbounded
-                behind = behind || !(cn[k] * Q.nd > 0.f);
-                const float lam = __fdividef(Q.nd, cn[k]);
-                const float u = __fmaf_rn(lam, cu[k], Q.base_u);
-                const float w = __fmaf_rn(lam, cv[k], Q.base_v);
+                behind = behind || !(cn[k] * s_nd.w > 0.f);
+                const float lam = __fdividef(s_nd.w, cn[k]);
+                const float u = __fmaf_rn(lam, cu[k], n_bu.w);
+                const float w = __fmaf_rn(lam, cv[k], eu_bv.w);
                 umin = fminf(umin, u);
                 umax = fmaxf(umax, u);
                 vmin = fminf(vmin, w);
                 vmax = fmaxf(vmax, w);
             }
+            const int4 dims = sp[p].dims;
+            const longlong2 fu = sp[p].first_us;
+            const int64_t v_stride = sp[p].vs.x;
             int u0, u1, v0, v1;
-            if (behind) {
+            if (!active) {  // no voxel: no candidates
                 u0 = 0;
-                u1 = Q.n_u - 1;
+                u1 = -1;
                 v0 = 0;
-                v1 = Q.n_v - 1;
+                v1 = -1;
+            } else if (behind) {
+                u0 = 0;
+                u1 = dims.x - 1;
+                v0 = 0;
+                v1 = dims.y - 1;
             } else {
                 u0 = max(0, (int)ceilf(umin - margin));
-                u1 = min(Q.n_u - 1, (int)floorf(umax + margin));
+                u1 = min(dims.x - 1, (int)floorf(umax + margin));
                 v0 = max(0, (int)ceilf(vmin - margin));
-                v1 = min(Q.n_v - 1, (int)floorf(vmax + margin));
+                v1 = min(dims.y - 1, (int)floorf(vmax + margin));
             }
             for (int jv = v0; jv <= v1; ++jv) {
                 for (int ju = u0; ju <= u1; ++ju) {
-                    const int64_t r = Q.first_ray + (int64_t)jv * Q.v_stride + (int64_t)ju * Q.u_stride;
-                    const float yr = __ldg(y + r);
-                    if (yr == 0.f) continue;
-                    float len;
-                    if constexpr (TAB) {
+                    const int64_t r = fu.x + (int64_t)jv * v_stride + (int64_t)ju * fu.y;
+                    float yr, len;
+                    if constexpr (YT) {
+                        const float4 ra = __ldg(tab + 2 * r), rb = __ldg(tab + 2 * r + 1);
+                        yr = rb.w;  // 0 for a skipped ray
+                        if (yr == 0.f) continue;
+                        len = voxel_len_row(ra, rb, ijk);
+                    } else if constexpr (TAB) {
+                        yr = __ldg(y + r);
+                        if (yr == 0.f) continue;
                         const float4 ra = __ldg(tab + 2 * r);
                         if (!(ra.w > 0.f)) continue;
                         len = voxel_len_row(ra, __ldg(tab + 2 * r + 1), ijk);
                     } else {
+                        yr = __ldg(y + r);
+                        if (yr == 0.f) continue;
                         const RaySetup R = ray_setup(src, dst, r, A);
                         if (!R.live) continue;
                         len = voxel_len(R, ijk);
@@ -324,14 +350,19 @@ int gather_entry(const char* what, const float* sino, int64_t batch, int64_t n_r
     cudaStream_t st = as_stream(stream);
     const PanelDev* pd = reinterpret_cast<const PanelDev*>(panels);
     if (ray_table && n_ray > 0) {
+        // one sinogram: its y goes into the table with the rays' set-up
         const int64_t tb = std::min<int64_t>((n_ray + 255) / 256, 148 * 64);
-        gather_ray_table_kernel<<<(unsigned)tb, 256, 0, st>>>(src, dst, n_ray, M_inv, b,
+        gather_ray_table_kernel<<<(unsigned)tb, 256, 0, st>>>(src, dst, n_ray, M_inv, b, batch == 1 ? sino : nullptr,
                                                               static_cast<RayRow*>(ray_table));
-        gather3d_kernel<true><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
-            sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f,
-            static_cast<const float4*>(ray_table));
+        const float4* tab = static_cast<const float4*>(ray_table);
+        if (batch == 1)
+            gather3d_kernel<true, true><<<dim3((unsigned)blocks, 1), 256, 0, st>>>(
+                sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, tab);
+        else
+            gather3d_kernel<true, false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
+                sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, tab);
     } else {
-        gather3d_kernel<false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
+        gather3d_kernel<false, false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
             sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, nullptr);
     }
     return launch_status(what);

@@ -298,6 +298,35 @@ def test_deterministic_gather_adjoint():
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
 
 
+@pytest.mark.parametrize("pitch,det", [(0.6, (40, 32)), (0.08, (240, 200))])
+def test_gather_ray_table_one_sinogram(pitch, det):
+    """One sinogram: the ray table carries y with each ray's set-up.  The sums
+    equal the table-free entry's bitwise (two sinograms, y read apart from the
+    table: test_deterministic_gather_adjoint) and the atomic adjoint's up to
+    the order of the float additions, within the projector tolerance 1e-5:
+    the 0.08 mm detector puts about nine rows and columns of cells on a
+    voxel, ~300 rays through it.  The grid (23 x 19 x 15) leaves the last
+    block partly without voxels."""
+    from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.tomography import back_project_3d_gather_cuda, panels_from_grid
+    from ct_laboratory_b200.tomography._common import inverse
+    C = _c()
+    c = cone_case(n=(23, 19, 15), n_view=4, det=det, pitch=pitch, seed=5)
+    n_view, (nu, nv) = c["n_view"], c["det"]
+    src, dst, Mi, b, M = T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]), T(c["M"])
+    dims = [int(v) for v in c["dims"]]
+    panels = panels_from_grid(src, dst, [v * nu * nv for v in range(n_view)], nu, nv, 1, nu, device=DEV)
+    yt = T(c["y"])
+    g1 = back_project_3d_gather_cuda(yt, src, dst, M, b, *dims, panels)
+    g0 = torch.empty_like(g1)
+    N.call("ctlab_back_project_3d_gather", N.ptr(yt), 1, yt.shape[0], N.ptr(src), N.ptr(dst), N.ptr(M),
+           N.ptr(inverse(M)), N.ptr(b), *dims, N.ptr(panels), n_view, N.ptr(g0), N.stream_of(yt))
+    assert torch.equal(g0, g1)
+    opts = N.tiling(n_view, nv, nu, nv * nu, nu, 1, voxel_rule=N.VOXEL_CROSSING)
+    at = C.back_project_3d_on_the_fly_cuda(yt, src, dst, Mi, b, *dims, tiling=opts)[0]
+    assert float(g1.abs().max()) > 0 and rel_err(g1.cpu().numpy(), at.cpu().numpy()) < TOL
+
+
 def test_deterministic_module_backward():
     from ct_laboratory_b200 import ConeBeam3DProjector
     kw = dict(n_x=24, n_y=20, n_z=16, n_view=6, det_nx=32, det_ny=24, sid=100.0, sdd=150.0, det_spacing=0.8,
