@@ -1189,8 +1189,8 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
             const int n_in = __popc(__ballot_sync(kFullMask, buf[lane].t < t_stop) & gmask);
             const int n_cells = (W == 16 && fin) ? 0 : min(n_in + 1, W);
             if constexpr (ADJ) {
-                // y * |v| once per lane, times each parameter span: the same
-                // segment lengths as the forward's, multiplied in another order
+                // y * |v| once per lane, times each parameter span (the
+                // forward applies |v| once to its sum of spans instead)
 #pragma unroll 1
                 for (int q = 0; q < n_cells; q += kGroupAdj) {
                     CellGroup<kGroupAdj> g;
