@@ -345,16 +345,19 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             for (int k = 0; k < kEdge; ++k)
                 red_add_if(out + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
         }
+        // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998) times y;
+        // the crossing rule multiplies y * |v| once by each span t1 - t0.
+        const float yl = MID ? y : __fmul_rn(y, ray_len);
 #pragma unroll 1
         for (int it = 0; it < max_it; ++it) {
             float tm = tn[0];
 #pragma unroll
             for (int a = 1; a < NDIM; ++a) tm = fminf(tm, tn[a]);
             const float t1 = fminf(tm, t_exit);
-            // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998).
-            const float seg = __fmul_rn(__fsub_rn(t1, t_cur), ray_len);
+            const float span = __fsub_rn(t1, t_cur);
+            const float seg = MID ? __fmul_rn(span, ray_len) : span;
             const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
-            red_add_if(out + (unsigned)v, __fmul_rn(y, seg), seg > 0.f && v >= 0);
+            red_add_if(out + (unsigned)v, __fmul_rn(yl, seg), seg > 0.f && v >= 0);
             if (!(tm < t_exit)) break;
             t_cur = t1;
 #pragma unroll
@@ -530,13 +533,16 @@ __device__ __forceinline__ int major2_setup(Major2& W, const float* sw, const fl
 // One step of the adjoint walk: the rest of the current major slab, split at
 // the minor plane inside it (if any), scattered as y * length.  MID: each
 // segment's voxel is the reference's rounded world midpoint, indexed with
-// Gt's strides (the buffer walked).  Returns whether the walk is done.
+// Gt's strides (the buffer walked), and `y` is y; otherwise `y` is
+// y * |v|, multiplied by each parameter span.  Returns whether the walk is
+// done.
 template <bool MID>
 __device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o, float y, const Affine2& A,
                                                 const GridDims<2>& Gt) {
     const float te = fminf(W.tnM, W.t_exit);
     const float ts = fminf(W.tnm, te);
-    const float sa = __fmul_rn(__fsub_rn(ts, W.t_cur), W.ray_len);
+    const float da = __fsub_rn(ts, W.t_cur);
+    const float sa = MID ? __fmul_rn(da, W.ray_len) : da;
     int va = W.idx;
     bool pa = sa > 0.f;
     if constexpr (MID) {
@@ -549,7 +555,8 @@ __device__ __forceinline__ bool major2_adj_step(Major2& W, float* __restrict__ o
         W.pnm += W.psm;
         W.tnm = plane_t(W.pnm, W.sm, W.im);
     }
-    const float sb = __fmul_rn(__fsub_rn(te, ts), W.ray_len);
+    const float db = __fsub_rn(te, ts);
+    const float sb = MID ? __fmul_rn(db, W.ray_len) : db;
     int vb = W.idx;
     bool pb = sb > 0.f;
     if constexpr (MID) {
@@ -649,7 +656,8 @@ __device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, 
         return __fmul_rn(acc, W.ray_len);
     } else {
 #pragma unroll 1
-        for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step<false>(W, out, y, A, G);
+        const float yl = __fmul_rn(y, W.ray_len);
+        for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step<false>(W, out, yl, A, G);
         return 0.f;
     }
 }
@@ -714,9 +722,10 @@ __device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in
     // every step crosses one major plane: at most n_major + 1 steps per lane
     // (a walk ends by itself before `last`; the bound only guards the loop)
     const int last = walk ? delay + W.n_major + 1 : 0;
+    const float ys = MID || !walk ? y : __fmul_rn(y, W.ray_len);  // the step's scale (major2_adj_step)
 #pragma unroll 1
     for (int it = 0;; ++it) {
-        if (!done && it >= delay) done = major2_adj_step<MID>(W, o, y, A, Gt) || it >= last;
+        if (!done && it >= delay) done = major2_adj_step<MID>(W, o, ys, A, Gt) || it >= last;
         if (__all_sync(kFullMask, done)) break;
     }
     if constexpr (MID) {
