@@ -14,9 +14,9 @@
 // with every plane parameter t = (p - s) * (1/v) and the per-ray set-up
 // (s, 1/v, |v|) computed exactly as the walks in walk.cuh compute them (t_enter
 // and t_exit need not be: see RaySetup).
-// These are the crossing-rule walk's segment spans times |v|, bitwise the
-// lengths the atomic adjoint scatters with (the forward applies |v| to each
-// ray's sum instead, a rounding-level difference), so the result is the
+// These are the crossing-rule walk's parameter spans (bitwise) times |v|
+// (the atomic adjoint scatters (y * |v|) * span, the forward applies |v| to
+// each ray's sum of spans: rounding-level differences), so the result is the
 // transpose of that forward, accumulated in a fixed order (panel, then row,
 // then column): bitwise reproducible from run to run.
 //

@@ -147,8 +147,7 @@ typedef struct ctlab_panel {
 
 /* Deterministic adjoint by gathering: every voxel sums y[b, r] * len(r, voxel)
  * over the rays of each panel that can reach it, in a fixed order, with
- * len evaluated by the arithmetic of the crossing-rule walk (bitwise the
- * lengths the atomic crossing-rule adjoint scatters).  It is bitwise
+ * len the crossing-rule walk's parameter span (bitwise) times |v|.  It is bitwise
  * reproducible, and is the transpose of
  * ctlab_forward_project_3d_on_the_fly_ex with CTLAB_VOXEL_CROSSING.  No
  * counterpart in the reference (its adjoints all scatter with atomicAdd,

@@ -5,8 +5,9 @@ It gathers per pixel through the 3-D gather kernel, the image being the
 one-voxel-thick volume [n_row, n_col, 1] with the rays in its z = 0 plane,
 where the 3-D arithmetic reduces exactly to the 2-D walk's.  So it must be:
 bitwise reproducible from call to call; the crossing-rule atomic adjoint
-up to the order of the float additions (tolerance 1e-6 here, well inside
-the projector tolerance 1e-5); the transpose of the crossing-rule forward
+up to the rounding of the products (y * |v| * span grouped differently) and
+the order of the float additions (tolerance 1e-6 here, well inside the
+projector tolerance 1e-5); the transpose of the crossing-rule forward
 (<A x, y> = <x, A^T y> in FP64 accumulation to 1e-6); and what autograd
 returns as the gradient, bitwise.
 """
