@@ -75,6 +75,13 @@ struct Dims {
 #define CTLAB_TABLE_BLOCK 8
 #endif
 constexpr int kTableBlock = CTLAB_TABLE_BLOCK;
+// The compressed kernels load the next block's deltas before working the
+// current block (their latency hidden behind its arithmetic; the static
+// ring's uint16 forward 6.94 against 7.12 ms): 1, or each block when it is
+// reached: 0.
+#ifndef CTLAB_TABLE_PREFETCH
+#define CTLAB_TABLE_PREFETCH 1
+#endif
 
 template <int NDIM, bool ADJ>
 __global__ void __launch_bounds__(256) tvals_lane_kernel(const float* __restrict__ in, float* __restrict__ out,
@@ -109,7 +116,9 @@ __global__ void __launch_bounds__(256) tvals_lane_kernel(const float* __restrict
     bool more = !isinf(t0);
 #pragma unroll 1
     for (int i0 = 1; i0 < n_int && more; i0 += kTableBlock) {
-        // the block's entries loaded together (kTableBlock loads in flight)
+        // the block's entries loaded together (kTableBlock loads in flight;
+        // loading the next block ahead measured slower here, 7.25 against
+        // 6.64 ms on the static ring's forward)
         float tb[kTableBlock];
 #pragma unroll
         for (int q = 0; q < kTableBlock; ++q) tb[q] = (i0 + q < n_int) ? __ldg(row + i0 + q) : __int_as_float(0x7f800000);
@@ -178,17 +187,24 @@ __global__ void __launch_bounds__(256) compressed_lane_kernel(const float* __res
 #pragma unroll
     for (int a = 0; a < 3; ++a) p0[a] = __fmaf_rn(start, vw[a], sw[a]);
     unsigned k = 0;  // running sum of the deltas, in unsigned int as the reference
+    // a block's deltas are loaded together (kTableBlock loads in flight)
+    auto load_block = [&](int i, unsigned* d) {
+#pragma unroll
+        for (int q = 0; q < kTableBlock; ++q) d[q] = (i + q < n_int) ? (unsigned)__ldg(row + i + q) : 0u;
+    };
+    unsigned d[kTableBlock];
+    load_block(1, d);
 #pragma unroll 1
     for (int i0 = 1; i0 < n_int; i0 += kTableBlock) {
-        // the block's deltas loaded together (kTableBlock loads in flight)
-        unsigned d[kTableBlock];
+#if CTLAB_TABLE_PREFETCH
+        unsigned dn[kTableBlock];
+        load_block(i0 + kTableBlock, dn);
+#endif
         unsigned any = 0u;
 #pragma unroll
-        for (int q = 0; q < kTableBlock; ++q) {
-            d[q] = (i0 + q < n_int) ? (unsigned)__ldg(row + i0 + q) : 0u;
-            any |= d[q];
-        }
-        if (any == 0u) continue;  // t unchanged over the block (past the last hit): nothing to add
+        for (int q = 0; q < kTableBlock; ++q) any |= d[q];
+        // any == 0: t unchanged over the block (past the last hit), nothing to add
+        if (any != 0u) {
         int vq[kTableBlock];
         float lq[kTableBlock];
 #pragma unroll
@@ -232,6 +248,13 @@ __global__ void __launch_bounds__(256) compressed_lane_kernel(const float* __res
             for (int q = 0; q < kTableBlock; ++q)
                 if (vq[q] >= 0) acc = __fmaf_rn(g[q], lq[q], acc);
         }
+        }
+#if CTLAB_TABLE_PREFETCH
+#pragma unroll
+        for (int q = 0; q < kTableBlock; ++q) d[q] = dn[q];
+#else
+        load_block(i0 + kTableBlock, d);
+#endif
     }
     if constexpr (!ADJ) out[bi * n_ray + r] = acc;
 }
