@@ -215,21 +215,19 @@ __device__ __forceinline__ void corner_values(float x0, const float4 h, float* o
 // whose footprints share detector columns).  The panels are taken in chunks
 // staged in shared memory; every thread of the block takes part in staging,
 // voxels past the grid included (with no candidates).
-// TAB: the rays' set-up comes from the ray table (tab), else it is
-// recomputed for every candidate; the lengths are the same bitwise.  YT: y
-// comes from the table too (one sinogram), so a candidate is one 32-byte
-// sector.  (Staging a warp's candidate rows in shared memory first, read
+// TAB: the rays' set-up and y come from the ray table (tab, built for the
+// sinogram gathered), so a candidate is one 32-byte sector; else the set-up
+// is recomputed for every candidate.  The lengths are the same bitwise.  (Staging a warp's candidate rows in shared memory first, read
 // coalesced along detector rows, measured slower: 97.8 against 82.8 ms on
 // the cone256 scan; each row is read by every warp whose voxels it crosses
 // either way.)
-template <bool TAB, bool YT>
+template <bool TAB>
 __global__ void __launch_bounds__(256, TAB ? 4 : 3) gather3d_kernel(const float* __restrict__ sino, float* __restrict__ out,
                                                        const float* __restrict__ src, const float* __restrict__ dst,
                                                        int64_t n_ray, const float* __restrict__ M_inv,
                                                        const float* __restrict__ bvec, const float* __restrict__ M,
                                                        int nx, int ny, int nz, const PanelDev* __restrict__ panels,
                                                        int n_panel, float margin, const float4* __restrict__ tab) {
-    static_assert(TAB || !YT, "y in the table needs the table");
     __shared__ PanelProj sp[kPanelChunk];
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nvox = (int64_t)nx * ny * nz;
@@ -300,17 +298,11 @@ __global__ void __launch_bounds__(256, TAB ? 4 : 3) gather3d_kernel(const float*
                 for (int ju = u0; ju <= u1; ++ju) {
                     const int64_t r = fu.x + (int64_t)jv * v_stride + (int64_t)ju * fu.y;
                     float yr, len;
-                    if constexpr (YT) {
+                    if constexpr (TAB) {
                         const float4 ra = __ldg(tab + 2 * r), rb = __ldg(tab + 2 * r + 1);
                         yr = rb.w;  // 0 for a skipped ray
                         if (yr == 0.f) continue;
                         len = voxel_len_row(ra, rb, ijk);
-                    } else if constexpr (TAB) {
-                        yr = __ldg(y + r);
-                        if (yr == 0.f) continue;
-                        const float4 ra = __ldg(tab + 2 * r);
-                        if (!(ra.w > 0.f)) continue;
-                        len = voxel_len_row(ra, __ldg(tab + 2 * r + 1), ijk);
                     } else {
                         yr = __ldg(y + r);
                         if (yr == 0.f) continue;
@@ -350,19 +342,20 @@ int gather_entry(const char* what, const float* sino, int64_t batch, int64_t n_r
     cudaStream_t st = as_stream(stream);
     const PanelDev* pd = reinterpret_cast<const PanelDev*>(panels);
     if (ray_table && n_ray > 0) {
-        // one sinogram: its y goes into the table with the rays' set-up
+        // sinogram by sinogram: its y goes into the table with the rays'
+        // set-up (rebuilt per sinogram, about 1 % of a gather), so that a
+        // candidate ray is one sector
         const int64_t tb = std::min<int64_t>((n_ray + 255) / 256, 148 * 64);
-        gather_ray_table_kernel<<<(unsigned)tb, 256, 0, st>>>(src, dst, n_ray, M_inv, b, batch == 1 ? sino : nullptr,
-                                                              static_cast<RayRow*>(ray_table));
         const float4* tab = static_cast<const float4*>(ray_table);
-        if (batch == 1)
-            gather3d_kernel<true, true><<<dim3((unsigned)blocks, 1), 256, 0, st>>>(
-                sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, tab);
-        else
-            gather3d_kernel<true, false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
-                sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, tab);
+        for (int64_t k = 0; k < batch; ++k) {
+            gather_ray_table_kernel<<<(unsigned)tb, 256, 0, st>>>(src, dst, n_ray, M_inv, b, sino + k * n_ray,
+                                                                  static_cast<RayRow*>(ray_table));
+            gather3d_kernel<true><<<dim3((unsigned)blocks, 1), 256, 0, st>>>(
+                sino + k * n_ray, out + k * nvox, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd,
+                (int)n_panel, 0.05f, tab);
+        }
     } else {
-        gather3d_kernel<false, false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
+        gather3d_kernel<false><<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(
             sino, out, src, dst, n_ray, M_inv, b, M, (int)n_x, (int)n_y, (int)n_z, pd, (int)n_panel, 0.05f, nullptr);
     }
     return launch_status(what);

@@ -655,8 +655,8 @@ __device__ __forceinline__ float traverse_major2(const float* __restrict__ vol, 
         }
         return __fmul_rn(acc, W.ray_len);
     } else {
-#pragma unroll 1
         const float yl = __fmul_rn(y, W.ray_len);
+#pragma unroll 1
         for (int it = 0; it < max_it && !done; ++it) done = major2_adj_step<false>(W, out, yl, A, G);
         return 0.f;
     }
