@@ -160,8 +160,9 @@ int ctlab_back_project_3d_gather(const float* sino, int64_t batch, int64_t n_ray
 /* ctlab_back_project_3d_gather with a caller-provided device workspace
  * `ray_table` of 32 * n_ray bytes, 16-byte aligned (NULL: as
  * ctlab_back_project_3d_gather): each ray's set-up (its source in index
- * space, 1/v and |v|) is computed into it once instead of once per voxel that
- * the ray can reach.  The result is bitwise the same. */
+ * space, 1/v and |v|) and its y are written into it once per sinogram
+ * instead of recomputed by every voxel that the ray can reach.  The result
+ * is bitwise the same. */
 int ctlab_back_project_3d_gather_ws(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                     const float* dst, const float* M, const float* M_inv, const float* b, int64_t n_x,
                                     int64_t n_y, int64_t n_z, const ctlab_panel* panels, int64_t n_panel, float* out,
