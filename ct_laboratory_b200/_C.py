@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import torch
 
+from . import _layout
 from . import _native as N
 
 __all__ = [
@@ -240,10 +241,15 @@ def back_project_3d_compressed_cuda(sino, t_uint16, t_start, t_scale, src, dst, 
 
 def forward_project_3d_on_the_fly_cuda(volume, src, dst, M_inv, b, tiling=None):
     """src/ct_projector_3d.cu:1018-1049 -> [batch, n_ray].  `tiling` (an
-    _native.RayTiling) is an optional launch-shape hint, not in the reference."""
+    _native.RayOpts) is an optional launch-shape hint, not in the reference;
+    without one the detector layout of src / dst is detected once per
+    geometry (_layout.detect_tiling) and the reference's midpoint voxel rule
+    is used."""
     _check_cuda("inputs must be CUDA", volume, src, dst)
     _f32c("volume", volume)
     _geom(src, dst, M_inv, b, 3)
+    if tiling is None:
+        tiling = _layout.detect_tiling(src, dst)
     batch, (n_x, n_y, n_z) = _vol_shape(volume, 3)
     n_ray = src.shape[0]
     out = torch.empty((batch, n_ray), device=volume.device, dtype=torch.float32)
@@ -254,10 +260,13 @@ def forward_project_3d_on_the_fly_cuda(volume, src, dst, M_inv, b, tiling=None):
 
 
 def back_project_3d_on_the_fly_cuda(sino, src, dst, M_inv, b, n_x, n_y, n_z, tiling=None):
-    """src/ct_projector_3d.cu:1051-1079 -> [batch, n_x, n_y, n_z]."""
+    """src/ct_projector_3d.cu:1051-1079 -> [batch, n_x, n_y, n_z]; `tiling` as
+    for the forward."""
     _check_cuda("inputs must be CUDA", sino, src, dst)
     _f32c("sinogram", sino)
     _geom(src, dst, M_inv, b, 3)
+    if tiling is None:
+        tiling = _layout.detect_tiling(src, dst)
     batch, n_ray = _sino_shape(sino)
     out = torch.empty((batch, n_x, n_y, n_z), device=sino.device, dtype=torch.float32)
     with torch.cuda.device(sino.device):

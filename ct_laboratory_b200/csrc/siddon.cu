@@ -75,6 +75,52 @@ __global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
     shared_xy_ray<ADJ, NB, W>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), b0, nb, cells[threadIdx.x >> 5]);
 }
 
+// The same launch shape under the reference's midpoint rule
+// (shared_xy_ray_mid): per warp the round's crossing parameters and its
+// certified cell records.
+template <bool ADJ, int NB, int W = 32>
+__global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
+    siddon3d_shared_xy_mid_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                  const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
+                                  const float* __restrict__ M_inv, const float* __restrict__ bvec, GridDims<3> G,
+                                  int64_t nvox, Tiling T, int batch) {
+    __shared__ float raw[256 / 32][kChunk];
+    __shared__ MidCell rec[256 / 32][kChunk];
+    const Affine3 A = load_affine3(M_inv, bvec);
+    const int64_t b0 = (int64_t)blockIdx.y * NB;
+    const int nb = min(NB, batch - (int)b0);
+    shared_xy_ray_mid<ADJ, NB, W>(in, out, src, dst, n_ray, A, G, nvox, tile_ray(T), b0, nb, raw[threadIdx.x >> 5],
+                                  rec[threadIdx.x >> 5]);
+}
+
+template <bool ADJ, bool MID, int NB, int W>
+static void launch_column(dim3 g, int threads, cudaStream_t s, const float* in, float* out, const float* src,
+                          const float* dst, int64_t n_ray, const float* M_inv, const float* b, const GridDims<3>& G,
+                          int64_t nvox, const Tiling& T, int batch) {
+    if constexpr (MID)
+        siddon3d_shared_xy_mid_kernel<ADJ, NB, W><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox,
+                                                                         T, batch);
+    else
+        siddon3d_shared_xy_kernel<ADJ, NB, W><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T,
+                                                                     batch);
+}
+
+// The column-walk kernel for nb volumes per walk and 32- or 16-row columns.
+template <bool ADJ, bool MID>
+static void launch_column_nb(int nb, int rows, dim3 g, int threads, cudaStream_t s, const float* in, float* out,
+                             const float* src, const float* dst, int64_t n_ray, const float* M_inv, const float* b,
+                             const GridDims<3>& G, int64_t nvox, const Tiling& T, int batch) {
+    if (rows == 16) {  // 16 detector rows per column: two 16-lane groups per warp
+        if (nb == 4) launch_column<ADJ, MID, 4, 16>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+        else if (nb == 2) launch_column<ADJ, MID, 2, 16>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+        else launch_column<ADJ, MID, 1, 16>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+        return;
+    }
+    if (nb == 4) launch_column<ADJ, MID, 4, 32>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+    else if (nb == 2) launch_column<ADJ, MID, 2, 32>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+    else launch_column<ADJ, MID, 1, 32>(g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T, batch);
+}
+
 
 // ----------------------------------------------------------------------------
 // host side
@@ -121,31 +167,23 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     const bool flat = tiling == nullptr || tiling->n_view == 0;
     const int walk = tiling == nullptr ? CTLAB_WALK_AUTO : tiling->walk;
     if constexpr (NDIM == 3) {
-        // Detector-row tilings (a warp = 32 rows of one column) under the
-        // crossing rule take the shared x-y walk; it checks per warp that the
-        // lanes share their x-y line and otherwise runs the per-lane walk.
+        // Detector-row tilings (a warp = 32 rows of one column, or two groups
+        // of 16) take the shared x-y walk under either voxel rule; it checks
+        // per warp that the lanes share their x-y line (and, under the
+        // midpoint rule, that M^-1 is diagonal) and otherwise runs the
+        // per-lane walk.
         const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
-        if (!flat && !mid && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
+        if (!flat && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
             (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
             const int nb = batch >= 4 ? 4 : (batch >= 2 ? 2 : 1);
             const dim3 g((unsigned)T.n_blocks, (unsigned)((batch + nb - 1) / nb));
-            const int bt = (int)batch;
-            if (T.tile_rows == 16) {
-                // 16 detector rows per column: two 16-lane groups per warp
-                if (nb == 4)
-                    siddon3d_shared_xy_kernel<ADJ, 4, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
-                else if (nb == 2)
-                    siddon3d_shared_xy_kernel<ADJ, 2, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
-                else
-                    siddon3d_shared_xy_kernel<ADJ, 1, 16><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
-                return launch_status(what);
-            }
-            if (nb == 4)
-                siddon3d_shared_xy_kernel<ADJ, 4><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
-            else if (nb == 2)
-                siddon3d_shared_xy_kernel<ADJ, 2><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+            const int rows = T.tile_rows == 16 ? 16 : 32;
+            if (mid)
+                launch_column_nb<ADJ, true>(nb, rows, g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T,
+                                            (int)batch);
             else
-                siddon3d_shared_xy_kernel<ADJ, 1><<<g, threads, 0, s>>>(in, out, src, dst, n_ray, M_inv, b, G, nvox, T, bt);
+                launch_column_nb<ADJ, false>(nb, rows, g, threads, s, in, out, src, dst, n_ray, M_inv, b, G, nvox, T,
+                                             (int)batch);
             return launch_status(what);
         }
     }

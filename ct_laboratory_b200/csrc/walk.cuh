@@ -1258,4 +1258,412 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     }
 }
 
+
+// ----------------------------------------------------------------------------
+// Shared x-y walk under the reference's midpoint rule (3-D).
+//
+// The reference charges each segment [t0, t1] to the voxel of its rounded
+// world-space midpoint s + tm v, tm = 0.5 (t0 + t1) (ct_projector_3d.cu:
+// 982-996).  With a diagonal M^-1 (every off-diagonal entry exactly zero, as
+// standard_image_transform_3d builds it) each index depends on its own axis
+// only: i = rne(m00 (fma(tm, v_x, s_x) - b_x)), and likewise j and k, because
+// the zero products of world_to_index3 add exact zeros.  Each is a chain of
+// monotone roundings of tm, so i(tm), j(tm) and k(tm) are monotone in tm.
+//
+// Lanes that share their world x-y line (one source, one detector column)
+// share every x- and y-plane parameter and every value of i(tm), j(tm).  The
+// warp derives the merged x-y crossings as in shared_xy_ray, and for each
+// cell [c0, c1] one lane evaluates (i, j) at the cell's midpoint and at
+// lo = c0 + delta and hi = c1 - delta: equal indices at lo, tm and hi prove,
+// by monotonicity, that every midpoint in [lo, hi] rounds to the same (i, j)
+// (a cell whose ends disagree shrinks that side of the interval to tm).  The
+// cell record holds c1, the flat (i, j) offset and [lo, hi].
+//
+// Each lane then walks its own segments, one per step: the segment ends at
+// the nearer of the cell end and its own next z plane, and the cell cursor
+// and the z plane advance as they are reached (several z planes per cell are
+// fine).  A segment's midpoint tm is formed as the reference forms it; inside
+// the cell's [lo, hi] its (i, j) is the record's and k = k(tm) is evaluated
+// directly; outside (a midpoint within delta of an x-y crossing) the voxel is
+// evaluated in full (midpoint_voxel), so every segment gets the reference's
+// voxel.  The segments just outside the grid whose midpoint rounds onto a face
+// voxel are added from edge_segments, as in traverse<3, ADJ, true>.  The
+// forward sums vol * ((t1 - t0) |v|) in walk order, the reference's terms in
+// the reference's order, so it is bitwise the reference's line integral.
+// ----------------------------------------------------------------------------
+struct __align__(16) MidCell {
+    float t;       // parameter of the crossing that ends the cell
+    int col;       // flat (i, j) offset of the rounded midpoint of the cell (k = 0)
+    float lo, hi;  // every midpoint parameter in [lo, hi] rounds to `col` in x and y
+};
+
+// Margin of the certified interval, 2^-K times the index-space magnitude over
+// |v| of the crossing axis (a few times the rounding noise of a plane
+// crossing); the certificate, not the margin, makes the interval exact.
+#ifndef CTLAB_MID_MARGIN_LOG2
+#define CTLAB_MID_MARGIN_LOG2 22
+#endif
+
+// (i, j) offset of the rounded world midpoint at parameter tm along a
+// diagonal affine; ok = inside the grid in x and y.
+struct XYMidLine {
+    float sx, sy, vx, vy, bx, by, mx, my;
+    int nx, ny, stx, sty;
+};
+
+__device__ __forceinline__ int xy_mid_offset(const XYMidLine& L, float tm, bool& ok) {
+    const int i = rne_int(__fmul_rn(L.mx, __fsub_rn(__fmaf_rn(tm, L.vx, L.sx), L.bx)));
+    const int j = rne_int(__fmul_rn(L.my, __fsub_rn(__fmaf_rn(tm, L.vy, L.sy), L.by)));
+    ok = (unsigned)i < (unsigned)L.nx && (unsigned)j < (unsigned)L.ny;
+    return i * L.stx + j * L.sty;
+}
+
+__device__ __forceinline__ bool affine_is_diagonal(const Affine3& A) {
+    return A.m[1] == 0.f && A.m[2] == 0.f && A.m[3] == 0.f && A.m[5] == 0.f && A.m[6] == 0.f && A.m[7] == 0.f;
+}
+
+// Per-lane slab-plane coordinates at parameter t for the edge segments:
+// behind (DIR = -1) or ahead (DIR = +1) of the slab holding t, per axis.
+template <int DIR>
+__device__ __forceinline__ void edge_planes(const LaneRay& R, float t, const GridDims<3>& G, float* p, float* ps) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        ps[a] = R.inv[a] == 0.f ? 0.f : (R.va[a] > 0.f ? 1.f : -1.f);
+        p[a] = 0.f;
+        if (R.inv[a] != 0.f) {
+            const int i = slab_at(t, R.s[a], R.va[a], R.inv[a], G.n[a]);
+            p[a] = (float)i + 0.5f * (float)DIR * ps[a];
+        }
+    }
+}
+
+// Segments walked per step of the midpoint walk (forward: gathers in flight).
+#ifndef CTLAB_MID_GROUP_FWD
+#define CTLAB_MID_GROUP_FWD 8
+#endif
+#ifndef CTLAB_MID_GROUP_ADJ
+#define CTLAB_MID_GROUP_ADJ 4
+#endif
+
+// Per-thread body; arguments as shared_xy_ray.  `raw` is the warp's kChunk
+// floats of crossing parameters, `rec` its kChunk cell records.
+template <bool ADJ, int NB, int W = 32>
+__device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, float* __restrict__ out,
+                                                  const float* __restrict__ src, const float* __restrict__ dst,
+                                                  int64_t n_ray, const Affine3& A, const GridDims<3>& G,
+                                                  int64_t nvox, int64_t r, int64_t b0, int nb, float* raw,
+                                                  MidCell* rec) {
+    static_assert(W == 32 || W == 16, "group width must be 32 or 16");
+    const int wlane = threadIdx.x & 31;
+    const int lane = wlane & (W - 1);
+    const unsigned gmask = W == 32 ? kFullMask : (0xffffu << (wlane & 16));
+    raw += wlane & (32 - W);
+    rec += wlane & (32 - W);
+    float sw[3] = {0.f, 0.f, 0.f}, dw[3] = {0.f, 0.f, 0.f};
+    if (r >= 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            sw[a] = ld_stream(src + r * 3 + a);
+            dw[a] = ld_stream(dst + r * 3 + a);
+        }
+    }
+    float y[NB];
+    bool any_y = false;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        y[j] = 0.f;
+        if constexpr (ADJ) {
+            if (r >= 0 && j < nb) y[j] = ld_stream(in + (b0 + j) * n_ray + r);
+        }
+        any_y = any_y || y[j] != 0.f;
+    }
+    LaneRay R;
+    lane_setup(R, sw, dw, G, A);
+    R.live = R.live && (r >= 0) && (!ADJ || any_y);
+
+    const unsigned warp_live = __ballot_sync(kFullMask, R.live);
+    const unsigned live_mask = warp_live & gmask;
+    if (warp_live == 0u) {
+        if (!ADJ && r >= 0) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, 0.f);
+        }
+        return;
+    }
+    // Do the live lanes share their world x-y line (source and detector cell
+    // in x and y), and is M^-1 diagonal?  (Dead lanes do not vote.)
+    const int leader = live_mask ? __ffs(live_mask) - 1 : (wlane & (32 - W));
+    const float sx = __shfl_sync(kFullMask, sw[0], leader), sy = __shfl_sync(kFullMask, sw[1], leader);
+    const float dx = __shfl_sync(kFullMask, dw[0], leader), dy = __shfl_sync(kFullMask, dw[1], leader);
+    const float s0 = __shfl_sync(kFullMask, R.s[0], leader), s1 = __shfl_sync(kFullMask, R.s[1], leader);
+    const float va0 = __shfl_sync(kFullMask, R.va[0], leader), va1 = __shfl_sync(kFullMask, R.va[1], leader);
+    const float i0 = __shfl_sync(kFullMask, R.inv[0], leader), i1 = __shfl_sync(kFullMask, R.inv[1], leader);
+    const float vxy = fmaxf(i0 != 0.f ? fabsf(va0) : 0.f, i1 != 0.f ? fabsf(va1) : 0.f);
+    const bool ok = !R.live || (__float_as_uint(sw[0]) == __float_as_uint(sx) &&
+                                __float_as_uint(sw[1]) == __float_as_uint(sy) &&
+                                __float_as_uint(dw[0]) == __float_as_uint(dx) &&
+                                __float_as_uint(dw[1]) == __float_as_uint(dy));
+    if (!affine_is_diagonal(A) || !__all_sync(kFullMask, ok && (live_mask == 0u || vxy != 0.f))) {
+        if (r < 0) return;
+#pragma unroll 1
+        for (int j = 0; j < nb; ++j) {  // the per-lane walk, once per volume
+            const int64_t b = b0 + j;
+            if constexpr (ADJ) {
+                const float yj = ld_stream(in + b * n_ray + r);
+                if (R.live && yj != 0.f)
+                    traverse<3, true, true>(nullptr, out + b * nvox, yj, sw, dw, G, A, (unsigned)nvox);
+            } else {
+                st_stream(out + b * n_ray + r,
+                          R.live ? traverse<3, false, true>(in + b * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
+                                 : 0.f);
+            }
+        }
+        return;
+    }
+    float vw[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vw[a] = __fsub_rn(dw[a], sw[a]);
+
+    // ---- x-y start, warp-uniform: the next planes after the earliest entry
+    const float kInf = __int_as_float(0x7f800000);
+    float t_start = R.live ? R.t_enter : kInf, t_stop = R.live ? R.t_exit : -kInf;
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) {
+        t_start = fminf(t_start, __shfl_xor_sync(kFullMask, t_start, o));
+        t_stop = fmaxf(t_stop, __shfl_xor_sync(kFullMask, t_stop, o));
+    }
+    float pnx = 0.f, pny = 0.f, psx = 0.f, psy = 0.f;
+    if (i0 != 0.f) {
+        psx = va0 > 0.f ? 1.f : -1.f;
+        pnx = (float)slab_at(t_start, s0, va0, i0, G.n[0]) + 0.5f * psx;
+    }
+    if (i1 != 0.f) {
+        psy = va1 > 0.f ? 1.f : -1.f;
+        pny = (float)slab_at(t_start, s1, va1, i1, G.n[1]) + 0.5f * psy;
+    }
+    XYMidLine L;
+    L.sx = sx;
+    L.sy = sy;
+    L.vx = __fsub_rn(dx, sx);
+    L.vy = __fsub_rn(dy, sy);
+    L.bx = A.b[0];
+    L.by = A.b[1];
+    L.mx = A.m[0];
+    L.my = A.m[4];
+    L.nx = G.n[0];
+    L.ny = G.n[1];
+    L.stx = G.stride[0];
+    L.sty = G.stride[1];
+    // certification margin: the smaller of the x and y crossing noise
+    // estimates (index-space magnitude 2^-K / |v|), in parameter units
+    float delta = kInf;
+    {
+        const float kM = 1.f / (float)(1 << CTLAB_MID_MARGIN_LOG2);
+        const float magx = fabsf(A.m[0]) * (fabsf(sx) + fabsf(dx) + fabsf(A.b[0])) + fabsf(s0) +
+                           fabsf(__fadd_rn(s0, va0)) + (float)G.n[0];
+        const float magy = fabsf(A.m[4]) * (fabsf(sy) + fabsf(dy) + fabsf(A.b[1])) + fabsf(s1) +
+                           fabsf(__fadd_rn(s1, va1)) + (float)G.n[1];
+        if (i0 != 0.f) delta = fminf(delta, kM * magx * fabsf(i0));
+        if (i1 != 0.f) delta = fminf(delta, kM * magy * fabsf(i1));
+    }
+
+    // ---- per-lane state: z plane, segment start, constants of k(tm) -------
+    float t_cur = 0.f, t_end = 0.f, tnz = kInf, pnz = 0.f, psz = 0.f;
+    if (R.live) {
+        t_cur = R.t_enter;
+        t_end = R.t_exit;
+        if (R.inv[2] != 0.f) {
+            psz = R.va[2] > 0.f ? 1.f : -1.f;
+            pnz = (float)slab_at(t_cur, R.s[2], R.va[2], R.inv[2], G.n[2]) + 0.5f * psz;
+            tnz = plane_t(pnz, R.s[2], R.inv[2]);
+        }
+    }
+    const float s2 = R.s[2], i2 = R.inv[2];
+    const float zs0 = sw[2], zv = vw[2], zb = A.b[2], zm = A.m[8];
+    const unsigned nz = (unsigned)G.n[2];
+    const float len = R.ray_len;
+
+    const float* vol[NB];
+    float* vout[NB];
+    float acc[NB], yl[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        const int64_t b = b0 + (j < nb ? j : nb - 1);
+        vol[j] = ADJ ? nullptr : pin_ptr(in + b * nvox);
+        vout[j] = ADJ ? pin_ptr(out + b * nvox) : nullptr;
+        acc[j] = 0.f;
+        yl[j] = __fmul_rn(y[j], len);  // adjoint: y * |v|, times each parameter span
+    }
+    const uint64_t pol = l2_policy_keep();
+
+    // ---- segments just before the entry (ascending, as the reference sums)
+    if (R.live) {
+        float p0[3], ps[3], el[kEdge];
+        int ev[kEdge];
+        edge_planes<-1>(R, t_cur, G, p0, ps);
+        const int ne = edge_segments<3, -1>(A, sw, vw, R.s, R.inv, ps, p0, t_cur, len, G, ev, el);
+#pragma unroll
+        for (int k = kEdge - 1; k >= 0; --k) {
+            const bool use = k < ne && el[k] > 0.f;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if constexpr (ADJ) {
+                    red_add_if(vout[j] + (unsigned)ev[k], __fmul_rn(y[j], el[k]), use && (NB == 1 || j < nb));
+                } else {
+                    if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)ev[k], pol), el[k], acc[j]);
+                }
+            }
+        }
+    }
+
+    const float fl = (float)lane;
+    const int max_rounds = (G.n[0] + G.n[1] + 2) / W + 2;
+    const int max_steps = W + G.n[2] + 2;  // cells of a round plus the z planes crossed in it
+    constexpr int kNG = ADJ ? CTLAB_MID_GROUP_ADJ : (CTLAB_MID_GROUP_FWD / NB > 0 ? CTLAB_MID_GROUP_FWD / NB : 1);
+    const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
+    float carry = t_start;  // start of the round's first cell
+    auto rounds = [&](auto uni_tag) {
+        constexpr bool UNI = decltype(uni_tag)::value;
+        bool fin = false;  // W = 16: this group has walked its last cell
+#pragma unroll 1
+        for (int round = 0; round < max_rounds; ++round) {
+            float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
+            float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
+            const int ky = warp_rank<false, W>(ty, tx);
+            const int kx = warp_rank<true, W>(tx, ty);
+            const int rx = lane + ky;
+            const int ry = lane + kx;
+            if (UNI) {
+                tx = fminf(tx, t_stop);
+                ty = fminf(ty, t_stop);
+            }
+            if (rx < W) raw[rx] = tx;
+            if (ry < W) raw[ry] = ty;
+            const int n_x = __popc(__ballot_sync(kFullMask, rx < W) & gmask);
+            __syncwarp();
+            const float c1 = raw[lane];
+            const float c0 = lane == 0 ? carry : raw[lane - 1];
+            const int n_in = __popc(__ballot_sync(kFullMask, c1 < t_stop) & gmask);
+            const int n_cells = (W == 16 && fin) ? 0 : min(n_in + 1, W);
+            carry = __shfl_sync(kFullMask, c1, (wlane & (32 - W)) + W - 1);
+            // the record of this lane's cell
+            {
+                const float tm = __fmul_rn(0.5f, __fadd_rn(c0, c1));
+                bool okm, okl, okh;
+                const int col = xy_mid_offset(L, tm, okm);
+                const float d = fmaxf(delta, c1 * (1.f / 2097152.f));
+                float lo = fminf(__fadd_rn(c0, d), tm), hi = fmaxf(__fsub_rn(c1, d), tm);
+                if (xy_mid_offset(L, lo, okl) != col || okl != okm) lo = tm;
+                if (xy_mid_offset(L, hi, okh) != col || okh != okm) hi = tm;
+                if (!okm) {  // midpoint outside the grid in x or y: every segment takes the full evaluation
+                    lo = kInf;
+                    hi = -kInf;
+                }
+                rec[lane] = MidCell{c1, col, lo, hi};
+            }
+            __syncwarp();
+            int q = 0;  // this lane's cell
+#pragma unroll 1
+            for (int st = 0; st < max_steps && __any_sync(kFullMask, q < n_cells); st += kNG) {
+                int vq[kNG];
+                float lq[kNG];
+                bool uq[kNG];
+#pragma unroll
+                for (int u = 0; u < kNG; ++u) {
+                    const bool active = q < n_cells;
+                    const MidCell c = rec[q < W ? q : W - 1];
+                    const float te = UNI ? c.t : fminf(c.t, t_end);
+                    const float t1 = fminf(tnz, te);
+                    const float span = __fsub_rn(t1, t_cur);
+                    const bool pos = active && span > 0.f;
+                    const float tm = __fmul_rn(0.5f, __fadd_rn(t_cur, t1));
+                    const int k = rne_int(__fmul_rn(zm, __fsub_rn(__fmaf_rn(tm, zv, zs0), zb)));
+                    const bool in_xy = tm >= c.lo && tm <= c.hi;
+                    int v = c.col + k;
+                    bool use = pos && in_xy && (unsigned)k < nz;
+                    if (pos && !in_xy) {  // midpoint near an x-y crossing: the full evaluation
+                        v = midpoint_voxel<3>(A, sw, vw, t_cur, t1, G);
+                        use = v >= 0;
+                    }
+                    vq[u] = use ? v : 0;
+                    uq[u] = use;
+                    lq[u] = ADJ ? span : __fmul_rn(span, len);
+                    if (active) {
+                        const bool zstep = tnz <= te, cstep = te <= tnz;
+                        if (zstep) {
+                            pnz += psz;
+                            tnz = plane_t(pnz, s2, i2);
+                        }
+                        q += cstep ? 1 : 0;
+                        t_cur = UNI ? t1 : fmaxf(t_cur, t1);
+                    }
+                    if constexpr (ADJ) {
+#pragma unroll
+                        for (int j = 0; j < NB; ++j)
+                            red_add_if(vout[j] + (unsigned)vq[u], __fmul_rn(yl[j], lq[u]),
+                                       uq[u] && (NB == 1 || j < nb));
+                    }
+                }
+                if constexpr (!ADJ) {
+                    float vv[NB][kNG];
+#pragma unroll
+                    for (int j = 0; j < NB; ++j)
+#pragma unroll
+                        for (int u = 0; u < kNG; ++u) vv[j][u] = uq[u] ? ld_keep(vol[j] + (unsigned)vq[u], pol) : 0.f;
+#pragma unroll
+                    for (int j = 0; j < NB; ++j)
+#pragma unroll
+                        for (int u = 0; u < kNG; ++u) acc[j] = uq[u] ? __fmaf_rn(vv[j][u], lq[u], acc[j]) : acc[j];
+                }
+            }
+            if constexpr (W == 32) {
+                if (n_in < W) break;
+            } else {
+                fin = fin || n_in < W;
+                if (__all_sync(kFullMask, fin)) break;
+            }
+            __syncwarp();  // every lane is done with this round's records
+            if (W == 32 || !fin) {
+                pnx = __fmaf_rn((float)n_x, psx, pnx);
+                pny = __fmaf_rn((float)(W - n_x), psy, pny);
+            }
+        }
+    };
+#if CTLAB_XY_UNIFORM
+    if (uniform) rounds(std::true_type{});
+    else
+#else
+    (void)uniform;
+#endif
+        rounds(std::false_type{});
+
+    // ---- segments just after the exit ----------------------------------------
+    if (R.live) {
+        float p0[3], ps[3], el[kEdge];
+        int ev[kEdge];
+        edge_planes<1>(R, t_end, G, p0, ps);
+        const int ne = edge_segments<3, 1>(A, sw, vw, R.s, R.inv, ps, p0, t_end, len, G, ev, el);
+#pragma unroll
+        for (int k = 0; k < kEdge; ++k) {
+            const bool use = k < ne && el[k] > 0.f;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                if constexpr (ADJ) {
+                    red_add_if(vout[j] + (unsigned)ev[k], __fmul_rn(y[j], el[k]), use && (NB == 1 || j < nb));
+                } else {
+                    if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)ev[k], pol), el[k], acc[j]);
+                }
+            }
+        }
+    }
+    if constexpr (!ADJ) {
+        if (r >= 0) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j)
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, acc[j]);
+        }
+    }
+}
+
 }  // namespace ctlab

@@ -168,12 +168,12 @@ class UniformStaticCTProjector3D(StaticCTProjector3D):
                  b_gantry, active_sources, modules_per_source, M, b, backend="cuda", precomputed_intersections=False,
                  tvals=None, use_compression=True, device: Optional[torch.device] = None, ray_tiling=None,
                  voxel_rule=0):
-        """voxel_rule 0 is the reference's midpoint rule; 1, the crossing
-        rule, also tiles the rays for the column walk (staticct_ray_tiling)
-        unless a ray_tiling is given."""
+        """voxel_rule 0 is the reference's midpoint rule, 1 the crossing
+        rule; either way the rays are tiled for the column walk
+        (staticct_ray_tiling) unless a ray_tiling is given."""
         if device is None:
             device = torch.device("cuda" if backend == "cuda" and torch.cuda.is_available() else "cpu")
-        if ray_tiling is None and voxel_rule == N.VOXEL_CROSSING:
+        if ray_tiling is None:
             n_view = int(torch.as_tensor(active_sources).sum()) * int(modules_per_source)
             ray_tiling = staticct_ray_tiling(n_view, det_nx_per_module, det_ny_per_module, voxel_rule=voxel_rule)
             if ray_tiling is None:
