@@ -240,12 +240,29 @@ def cpu_baseline(case, target_s=15.0, gpu_view0=None):
     return out
 
 
+def _workloads_standalone():
+    """workloads.py loaded by file path: the reference arm builds its rays and
+    phantom from the package's self-contained geometry and phantom files
+    without importing the package, so the only native libraries this process
+    maps are the oracle's."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_ctlab_workloads",
+                                                  os.path.join(ROOT, "ct_laboratory_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # (dataclasses look their module up there)
+    spec.loader.exec_module(mod)
+    return mod.WORKLOADS
+
+
 def run_reference(args, world, rank):
     """The reference's CPU projector on this host's cores (rank 0 only)."""
-    from ct_laboratory_b200.workloads import WORKLOADS
     if rank != 0:
         return
-    w = WORKLOADS[args.workload]
+    w = _workloads_standalone().get(args.workload)
+    if w is None or not w.name.startswith(("cone", "fan")):
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference CPU arm covers the cone-beam and "
+                                                              f"fan-beam workloads, not {args.workload}"}))
+        return
     case = CpuCase(w)
     threads = cpu_threads()
     rate, _, _ = case.rate([0], threads)
@@ -266,6 +283,7 @@ def run_reference(args, world, rank):
            "cpu_baseline": {"value": value, "unit": "GRays/s", "cores": threads, "kind": "port",
                             "sample": f"{n_views} views per step of {w.n_view}, rotating"},
            "e2e": {"value": value, "unit": "GRays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    assert "ct_laboratory_b200" not in sys.modules, "the reference arm must not import the package"
     print(json.dumps(out))
 
 

@@ -1,10 +1,8 @@
 """3-D cone-beam geometry and projector class.
 
-``build_conebeam_3d_geometry`` returns the same rays as the reference's
-(tomography/conebeam_projector_3d.py:6-96), evaluated with the same float32
-torch operations: circular source orbit of radius sid in the z = cz plane,
-flat detector at sdd - sid beyond the isocentre with u along the in-plane
-perpendicular and v along +z, rays ordered [view][det_v][det_u].
+``build_conebeam_3d_geometry`` (ct_laboratory_b200/ray_geometry.py) returns
+the same rays as the reference's (tomography/conebeam_projector_3d.py:6-96),
+ordered [view][det_v][det_u].
 
 ``ConeBeam3DProjector`` additionally passes the kernels a ray tiling with
 rows = det_v and cols = det_u, so that the 32 lanes of a warp trace 32
@@ -12,49 +10,15 @@ vertically adjacent rays (the same x-y path, neighbouring k voxels).
 """
 from __future__ import annotations
 
-import math
-
 import torch
 
 from .. import _native as N
+from ..ray_geometry import build_conebeam_3d_geometry
 from .ct_projector_3d_module import CTProjector3DModule
 from .gather import panels_from_grid
 from .standard_image_transform import standard_image_transform_3d
 
 __all__ = ["build_conebeam_3d_geometry", "ConeBeam3DProjector", "conebeam_tiling"]
-
-
-def build_conebeam_3d_geometry(n_view, det_nx, det_ny, sid, sdd, det_spacing=1.0, angle_offset=0.0,
-                               volume_center_xyz=(0.0, 0.0, 0.0), device=None):
-    """Rays of a circular cone-beam scan, [n_view * det_ny * det_nx, 3] each.
-    `device` (an addition; default the host, as the reference) builds them
-    directly on a GPU, where large scans take milliseconds instead of seconds
-    (the same formulas; the device's cos / sin may round differently)."""
-    cx, cy, cz = volume_center_xyz
-    ang = torch.linspace(0, 2 * math.pi - 2 * math.pi / n_view, n_view, dtype=torch.float32,
-                         device=device) + angle_offset
-    cos_t, sin_t = torch.cos(ang), torch.sin(ang)
-    view = lambda t: t.view(n_view, 1, 1)  # noqa: E731
-    sx, sy = view(cx + sid * cos_t), view(cy + sid * sin_t)
-    sz = torch.full_like(sx, cz)
-    dcx, dcy = view(cx - (sdd - sid) * cos_t), view(cy - (sdd - sid) * sin_t)
-    dcz = torch.full_like(dcx, cz)
-    # in-plane unit vector perpendicular to the central ray
-    px, py = -(dcy - sy), (dcx - sx)
-    norm = torch.sqrt(px * px + py * py)
-    px, py = px / norm, py / norm
-    pz = torch.zeros_like(px)
-    U = ((torch.arange(det_nx, dtype=torch.float32, device=device) - (det_nx - 1) / 2.0) * det_spacing) \
-        .unsqueeze(0).expand(det_ny, det_nx)
-    V = ((torch.arange(det_ny, dtype=torch.float32, device=device) - (det_ny - 1) / 2.0) * det_spacing) \
-        .unsqueeze(1).expand(det_ny, det_nx)
-    cell_x = dcx + px * U + 0.0 * V
-    cell_y = dcy + py * U + 0.0 * V
-    cell_z = dcz + pz * U + 1.0 * V
-    shape = (n_view, det_ny, det_nx)
-    src = torch.stack([sx.expand(shape), sy.expand(shape), sz.expand(shape)], dim=-1).reshape(-1, 3)
-    dst = torch.stack([cell_x, cell_y, cell_z], dim=-1).reshape(-1, 3)
-    return src, dst
 
 
 def conebeam_tiling(n_view, det_nx, det_ny, tile_rows=32, block_threads=128, voxel_rule=0, walk=0):

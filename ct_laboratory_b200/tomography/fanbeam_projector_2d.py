@@ -1,53 +1,19 @@
 """2-D fan-beam geometry and projector class.
 
-``build_fanbeam_2d_geometry`` returns the same rays as the reference's
-(tomography/fanbeam_projector_2d.py:6-82): view angles
-linspace(0, 2*pi - 2*pi/n_view, n_view) (float32) + offset, source at radius
-sid, flat detector centred at distance sdd - sid beyond the isocentre,
-cells (i - (n_det-1)/2) * spacing along the detector, rays ordered
-[view][cell].  Per-view quantities are evaluated in double precision and
-rounded to float32 once, as the reference's Python loop does; the cells of a
-view are evaluated as one numpy float64 vector instead of a Python loop.
+``build_fanbeam_2d_geometry`` (ct_laboratory_b200/ray_geometry.py) returns
+the same rays as the reference's (tomography/fanbeam_projector_2d.py:6-82),
+ordered [view][cell].
 """
 from __future__ import annotations
 
-import math
-
-import numpy as np
 import torch
 
+from ..ray_geometry import build_fanbeam_2d_geometry
 from .ct_projector_2d_module import CTProjector2DModule
 from .gather import panels_from_lines_2d
 from .standard_image_transform import standard_image_transform_2d
 
 __all__ = ["build_fanbeam_2d_geometry", "FanBeam2DProjector"]
-
-
-def build_fanbeam_2d_geometry(n_view, n_det, sid, sdd, det_spacing=1.0, angle_offset=0.0,
-                              image_center_xy=(0.0, 0.0)):
-    cx, cy = image_center_xy
-    angles = torch.linspace(0, 2 * math.pi - 2 * math.pi / n_view, n_view) + angle_offset
-    cell = (np.arange(n_det, dtype=np.float64) - (n_det - 1) / 2.0) * det_spacing
-    srcs, dsts = [], []
-    for theta in angles.tolist():
-        c, s = math.cos(theta), math.sin(theta)
-        sx, sy = cx + sid * c, cy + sid * s
-        dcx, dcy = cx - (sdd - sid) * c, cy - (sdd - sid) * s
-        px, py = -(dcy - sy), (dcx - sx)
-        norm = math.sqrt(px ** 2 + py ** 2)
-        if norm < 1e-12:
-            continue  # degenerate view
-        px, py = px / norm, py / norm
-        d = np.empty((n_det, 2), dtype=np.float64)
-        d[:, 0] = dcx + cell * px
-        d[:, 1] = dcy + cell * py
-        srcs.append(np.broadcast_to(np.array([sx, sy]), (n_det, 2)))
-        dsts.append(d)
-    if not srcs:
-        return torch.empty((0, 2), dtype=torch.float32), torch.empty((0, 2), dtype=torch.float32)
-    src = torch.from_numpy(np.ascontiguousarray(np.concatenate(srcs), dtype=np.float32))
-    dst = torch.from_numpy(np.ascontiguousarray(np.concatenate(dsts), dtype=np.float32))
-    return src, dst
 
 
 class FanBeam2DProjector(CTProjector2DModule):

@@ -22,9 +22,32 @@ serve    MAP reconstruction jobs arriving as a seeded Poisson process (mean
 """
 from __future__ import annotations
 
+import importlib
+import importlib.util
+import os
+import sys
 from dataclasses import dataclass
 
 __all__ = ["ConeWorkload", "FanWorkload", "ScanBatchWorkload", "ServingWorkload", "StaticRingWorkload", "WORKLOADS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _sibling(rel):
+    """A self-contained module of this package (ray_geometry, phantoms,
+    tomography/standard_image_transform): imported through the package when
+    this file was, else loaded by file path, so that a process that loads
+    this file by path (the reference CPU arm of bench.py) builds the
+    workloads' rays and phantoms without mapping the native library."""
+    if __package__:
+        return importlib.import_module(f"{__package__}." + rel.replace("/", "."))
+    name = "_ctlab_" + rel.replace("/", "_")
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(_HERE, rel + ".py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
 
 
 @dataclass(frozen=True)
@@ -46,15 +69,15 @@ class ConeWorkload:
         return self.n_view * self.det_nx * self.det_ny
 
     def geometry(self):
-        from .tomography import build_conebeam_3d_geometry, standard_image_transform_3d
-        src, dst = build_conebeam_3d_geometry(self.n_view, self.det_nx, self.det_ny, self.sid, self.sdd, self.pitch)
-        M, b = standard_image_transform_3d(*self.n, self.voxel, self.voxel, self.voxel)
+        src, dst = _sibling("ray_geometry").build_conebeam_3d_geometry(self.n_view, self.det_nx, self.det_ny,
+                                                                       self.sid, self.sdd, self.pitch)
+        M, b = _sibling("tomography/standard_image_transform").standard_image_transform_3d(
+            *self.n, self.voxel, self.voxel, self.voxel)
         return src, dst, M, b
 
     def phantom(self, device="cpu"):
-        from .phantoms import ellipsoid_phantom_3d
-        return ellipsoid_phantom_3d(*self.n, voxel=self.voxel, n_ellipsoid=self.n_ellipsoid, seed=self.seed,
-                                    device=device)
+        return _sibling("phantoms").ellipsoid_phantom_3d(*self.n, voxel=self.voxel, n_ellipsoid=self.n_ellipsoid,
+                                                         seed=self.seed, device=device)
 
 
 @dataclass(frozen=True)
@@ -74,14 +97,14 @@ class FanWorkload:
         return self.n_view * self.n_det
 
     def geometry(self):
-        from .tomography import build_fanbeam_2d_geometry, standard_image_transform_2d
-        src, dst = build_fanbeam_2d_geometry(self.n_view, self.n_det, self.sid, self.sdd, self.pitch)
-        M, b = standard_image_transform_2d(*self.n, self.pixel, self.pixel)
+        src, dst = _sibling("ray_geometry").build_fanbeam_2d_geometry(self.n_view, self.n_det, self.sid, self.sdd,
+                                                                      self.pitch)
+        M, b = _sibling("tomography/standard_image_transform").standard_image_transform_2d(*self.n, self.pixel,
+                                                                                          self.pixel)
         return src, dst, M, b
 
     def phantom(self, device="cpu"):
-        from .phantoms import ellipse_phantom_2d
-        return ellipse_phantom_2d(*self.n, pixel=self.pixel, seed=self.seed, device=device)
+        return _sibling("phantoms").ellipse_phantom_2d(*self.n, pixel=self.pixel, seed=self.seed, device=device)
 
 
 @dataclass(frozen=True)
