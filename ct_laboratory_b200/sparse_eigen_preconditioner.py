@@ -1,27 +1,35 @@
-"""Matrix-free leading eigenpairs of G = A^T A and the preconditioners built on them.
+"""Leading eigenpairs of G = A^T A, computed matrix-free on the GPU, and the
+preconditioners built on them.
 
-Mirrors the reference's sparse_eigen_preconditioner area
-(ct_laboratory/sparse_eigen_preconditioner/sparse_eigen_decomposition.py:39-366,
-preconditioners.py:28-138): ``SparseEigenDecomposition(projector, k)`` with
-``compute_weights(method=...)`` filling buffers ``s`` (singular values,
-descending), ``v`` (N x k image eigenvectors) and ``p`` (n_ray x k
-projection eigenvectors A v), ``save`` / ``load``, ``register_method``,
-``to_image_preconditioner`` / ``to_projection_preconditioner``; and the
-image- and projection-domain preconditioners
-    P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I.
+Public names and file formats follow the reference's sparse_eigen_preconditioner
+area (ct_laboratory/sparse_eigen_preconditioner/sparse_eigen_decomposition.py,
+preconditioners.py): ``SparseEigenDecomposition(operator, k)`` with
+``compute_weights(method=...)`` filling the buffers ``s`` (singular values
+sqrt(eig), descending), ``v`` ([N, k] image eigenvectors) and ``p`` ([n_ray,
+k] projection eigenvectors A v); ``save`` / ``load`` write and read the same
+checkpoint dict {"state_dict", "k", "volume_shape"}; ``register_method(name,
+fn)`` adds a solver ``fn(dec, gram, N, k, **kw) -> (eigenvalues, V)``; and the
+two preconditioners apply
 
-Solvers:
-  "subspace"  block power iteration + Rayleigh-Ritz, as the reference's
-  "eigsh"     SciPy ARPACK with the matvec on the GPU (one host round trip
-              per matvec, as the reference's)
-  "lanczos"   thick-restart Lanczos with full re-orthogonalisation, entirely
-              on the GPU: no host round trip per matvec.
-The Gram operator is applied to a block of columns with one batched forward
-and one batched adjoint launch (the reference applies it column by column,
-sparse_eigen_decomposition.py:120-128).
+    P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I      (P^2 ~ G^-1)
+
+through the image basis or through p = A V and the projector.
+
+How the work is organised here:
+  * the Gram operator is applied to a block of columns at once: the columns
+    go through the projector as one batch of volumes (one batched forward and
+    one batched adjoint launch per block, ``_GramOperator``);
+  * "subspace": subspace iteration with a Rayleigh-Ritz step on every sweep,
+    one block Gram application per sweep (the Ritz values of the current
+    basis come from the same product that advances it);
+  * "lanczos": thick-restart Lanczos with full re-orthogonalisation, all on
+    the device (no host round trip per matvec);
+  * "eigsh": SciPy's ARPACK driven from the host, one device Gram matvec per
+    ARPACK request.
 """
 from __future__ import annotations
 
+import math
 import time
 
 import torch
@@ -31,351 +39,394 @@ from .optimization import Preconditioner
 
 __all__ = ["SparseEigenDecomposition", "SparseEigenImagePreconditioner", "SparseEigenProjectionPreconditioner"]
 
+_BASIS = ("s", "v", "p")
+
+
+class _GramOperator:
+    """x -> A^T A x for flattened volumes, one vector or a block of columns.
+
+    Built from a projector (forward_project / back_project on [B, n_x, n_y,
+    n_z] batches) or from a user callable acting on one flattened vector."""
+
+    def __init__(self, projector, gram_fn, volume_shape, block):
+        self.projector = projector
+        self.gram_fn = gram_fn
+        self.volume_shape = volume_shape
+        self.block = block
+        self.count = 0
+
+    def vector(self, x):
+        self.count += 1
+        if self.gram_fn is not None:
+            return self.gram_fn(x).reshape(-1)
+        vol = x.reshape(self.volume_shape).contiguous()
+        with torch.no_grad():
+            return self.projector.back_project(self.projector.forward_project(vol)).reshape(-1)
+
+    def columns(self, Q):
+        """G Q for Q of shape [N, m]."""
+        if self.gram_fn is not None or self.projector is None:
+            return torch.stack([self.vector(q) for q in Q.unbind(dim=1)], dim=1)
+        m = Q.shape[1]
+        width = m if not self.block else max(1, int(self.block))
+        out = torch.empty_like(Q)
+        for lo in range(0, m, width):
+            hi = min(m, lo + width)
+            vols = Q[:, lo:hi].t().reshape(hi - lo, *self.volume_shape).contiguous()
+            with torch.no_grad():
+                g = self.projector.back_project(self.projector.forward_project(vols))
+            out[:, lo:hi] = g.reshape(hi - lo, -1).t()
+            self.count += hi - lo
+        return out
+
+
+def _resolve(operator, gram, volume_shape, device):
+    """(projector, forward callable, volume shape, device) from the
+    constructor's arguments: a projector object, a bare forward callable
+    (then volume_shape or gram is needed), or only a gram callable."""
+    if operator is None:
+        if gram is None:
+            raise ValueError("SparseEigenDecomposition needs a projector, a forward callable or a gram callable")
+        return None, None, volume_shape, device
+    if all(hasattr(operator, name) for name in ("forward_project", "back_project", "n_x", "n_y", "n_z")):
+        shape = (int(operator.n_x), int(operator.n_y), int(operator.n_z))
+        if device is None and isinstance(getattr(operator, "M", None), torch.Tensor):
+            device = operator.M.device
+        return operator, operator.forward_project, shape, device
+    if not callable(operator):
+        raise TypeError(f"operator must be a projector or a callable (got {type(operator).__name__})")
+    if volume_shape is None and gram is None:
+        raise ValueError("a bare forward callable needs volume_shape (or a gram callable)")
+    return None, operator, volume_shape, device
+
+
+def _sym(T):
+    return 0.5 * (T + T.t())
+
+
+def subspace_iteration(dec, gram, N, k, n_iters=30, tol=1e-6, seed=None, oversample=0, verbose=False, **_):
+    """k leading eigenpairs by subspace iteration.  Each sweep multiplies the
+    orthonormal basis Q by G once; the Ritz values of Q (eigenvalues of
+    Q^T G Q) decide convergence (relative change below `tol`), and the next
+    basis is the orthonormalised product.  The last basis's product gives the
+    final Rayleigh-Ritz pairs without another application of G."""
+    m = min(N, k + max(0, int(oversample)))
+    gen = torch.Generator(device="cpu")
+    if seed is not None:
+        gen.manual_seed(int(seed))
+    Q = torch.linalg.qr(torch.randn(N, m, generator=gen, dtype=dec.dtype).to(dec.device_))[0]
+    sweeps = max(1, int(n_iters))
+    last = None
+    for sweep in range(sweeps):
+        Z = gram(Q)
+        ritz = torch.linalg.eigvalsh(_sym(Q.t() @ Z))
+        if last is not None:
+            change = float((ritz - last).abs().max() / last.abs().max().clamp_min(1e-30))
+            if verbose:
+                print(f"  [subspace] sweep {sweep}: largest Ritz value {float(ritz[-1]):.4e}, change {change:.2e}")
+            if change < tol:
+                break
+        last = ritz
+        if sweep + 1 < sweeps:
+            Q = torch.linalg.qr(Z)[0]
+    theta, W = torch.linalg.eigh(_sym(Q.t() @ Z))
+    top = torch.flip(torch.arange(theta.numel(), device=theta.device), dims=[0])[:k]
+    return theta[top].clamp_min(0.0), Q @ W[:, top]
+
+
+def arpack_eigsh(dec, gram, N, k, tol=1e-3, maxiter=5000, seed=42, ncv=None, verbose=False, **_):
+    """k largest eigenpairs by SciPy's ARPACK (implicitly restarted Lanczos)
+    on the host; every matvec it asks for is one Gram application on the
+    device."""
+    import numpy as np
+    from scipy.sparse.linalg import LinearOperator, eigsh
+
+    def matvec(x):
+        xt = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).to(dec.device_, dec.dtype)
+        return dec._gram.vector(xt).float().cpu().numpy()
+
+    start = np.random.default_rng(None if seed is None else int(seed)).standard_normal(N).astype(np.float32)
+    vals, vecs = eigsh(LinearOperator((N, N), matvec=matvec, dtype=np.float32), k=k, which="LM", v0=start,
+                       tol=tol, maxiter=maxiter, ncv=ncv)
+    order = np.argsort(-vals)
+    if verbose:
+        print(f"  [eigsh] {dec._gram.count} matvecs")
+    return (torch.from_numpy(np.clip(vals[order], 0.0, None).copy()).to(dec.device_, dec.dtype),
+            torch.from_numpy(vecs[:, order].copy()).to(dec.device_, dec.dtype))
+
+
+def thick_restart_lanczos(dec, gram, N, k, tol=1e-3, ncv=None, max_restarts=50, seed=42, verbose=False, **_):
+    """k largest eigenpairs by thick-restart Lanczos, on the device.
+
+    Basis V ((ncv+1) x N, one vector per row, so that every product with it
+    reads whole contiguous vectors) in float32 with two passes of classical
+    Gram-Schmidt against all previous vectors per step; the projected matrix
+    T = V G V^T in float64.  After ncv vectors the k leading Ritz vectors and
+    the residual direction are kept and the iteration continues from them.
+    Converged when every kept Ritz pair has residual |beta s_last| <= tol
+    theta_max."""
+    dev, dt = dec.device_, dec.dtype
+    ncv = int(ncv) if ncv is not None else min(N - 1, max(20, 2 * k + 1))
+    if not (k < ncv < N):
+        raise ValueError("lanczos needs k < ncv < N")
+    gen = torch.Generator(device="cpu").manual_seed(int(seed))
+    V = torch.empty(ncv + 1, N, dtype=dt, device=dev)
+    v0 = torch.randn(N, generator=gen, dtype=dt).to(dev)
+    V[0] = v0 / v0.norm()
+    T = torch.zeros(ncv, ncv, dtype=torch.float64, device=dev)
+    start = 0
+    beta_last = torch.zeros((), dtype=dt, device=dev)
+    for restart in range(int(max_restarts)):
+        for j in range(start, ncv):
+            w = dec._gram.vector(V[j])
+            h = V[:j + 1] @ w
+            w = w - V[:j + 1].t() @ h
+            h2 = V[:j + 1] @ w
+            w = w - V[:j + 1].t() @ h2
+            h = (h + h2).double()
+            T[:j + 1, j] = h
+            T[j, :j + 1] = h
+            beta = w.norm()
+            if j + 1 < ncv:
+                T[j + 1, j] = T[j, j + 1] = beta.double()
+            V[j + 1] = w / beta.clamp_min(1e-30)
+            beta_last = beta
+        theta, S = torch.linalg.eigh(T)
+        order = torch.argsort(theta, descending=True)
+        theta, S = theta[order], S[:, order]
+        res = (beta_last.double() * S[-1, :k]).abs()
+        if verbose:
+            print(f"  [lanczos] restart {restart}: theta_max={float(theta[0]):.4e} "
+                  f"max residual/theta_max={float(res.max() / theta[0].abs()):.2e}")
+        if bool((res <= tol * theta[0].abs()).all()) or restart == max_restarts - 1:
+            break
+        Y = S[:, :k].t().to(dt) @ V[:ncv]
+        resid = V[ncv].clone()
+        V[:k] = Y
+        V[k] = resid
+        T.zero_()
+        T[:k, :k] = torch.diag(theta[:k])
+        coup = beta_last.double() * S[-1, :k]
+        T[k, :k] = coup
+        T[:k, k] = coup
+        start = k
+    Y = (S[:, :k].t().to(dt) @ V[:ncv]).t()
+    return torch.clamp(theta[:k], min=0.0).to(dt), Y
+
 
 class SparseEigenDecomposition(nn.Module):
-    _METHODS = {}
+    """Matrix-free leading eigen-decomposition of the Gram operator A^T A.
+
+    operator: a projector (forward_project, back_project, n_x, n_y, n_z), or
+    a bare forward callable (with volume_shape), or None with `gram`, a
+    callable x -> A^T A x on flattened volumes.  `block` bounds the columns
+    sent through the projector together (None: a whole basis at once)."""
+
+    _solvers = {}
 
     def __init__(self, operator=None, k=32, volume_shape=None, gram=None, dtype=None, device=None, block=None):
         super().__init__()
         self.k = int(k)
-        self._projector = None
-        self._forward = None
-        self._gram_user = gram
-        self.block = block  # columns per batched Gram application (None: all at once)
-        if gram is None and operator is None:
-            raise ValueError("provide either an `operator` (projector or forward callable) or a `gram` callable")
-        if hasattr(operator, "forward_project") and hasattr(operator, "back_project"):
-            self._projector = operator
-            self._forward = operator.forward_project
-            volume_shape = (operator.n_x, operator.n_y, operator.n_z)
-            if device is None and hasattr(operator, "M"):
-                device = operator.M.device
-        elif callable(operator):
-            if volume_shape is None and gram is None:
-                raise ValueError("`volume_shape` is required when `operator` is a bare forward callable")
-            self._forward = operator
-        self.volume_shape = tuple(volume_shape) if volume_shape is not None else None
+        self._projector, self._forward, shape, device = _resolve(operator, gram, volume_shape, device)
+        self.volume_shape = None if shape is None else tuple(int(n) for n in shape)
         self.dtype = dtype or torch.float32
-        self.device_ = device or torch.device("cpu")
-        self.register_buffer("s", torch.zeros(0, dtype=self.dtype))
-        self.register_buffer("v", torch.zeros(0, 0, dtype=self.dtype))
-        self.register_buffer("p", torch.zeros(0, dtype=self.dtype))
-        self.n_matvec = 0
+        self.device_ = torch.device(device) if device is not None else torch.device("cpu")
+        self._gram = _GramOperator(self._projector, gram, self.volume_shape, block)
+        self._install(None, None, None)
+        self.register_load_state_dict_pre_hook(SparseEigenDecomposition._reshape_for_load)
 
-    # -- operator plumbing ---------------------------------------------------
+    # -- basis storage --------------------------------------------------------
+    def _install(self, s, v, p):
+        empty = torch.zeros(0, dtype=self.dtype)
+        for name, t in zip(_BASIS, (s, v, p)):
+            self.register_buffer(name, empty.clone() if t is None else t.contiguous())
+
+    @staticmethod
+    def _reshape_for_load(module, state_dict, prefix, *_):
+        # the basis buffers take the checkpoint's shapes before the copy
+        for name in _BASIS:
+            if prefix + name in state_dict:
+                t = state_dict[prefix + name]
+                module.register_buffer(name, torch.empty(t.shape, dtype=t.dtype, device=getattr(module, name).device))
+
     @property
     def N(self):
         if self.volume_shape is not None:
-            n = 1
-            for d in self.volume_shape:
-                n *= d
-            return n
+            return math.prod(self.volume_shape)
         return self.v.shape[0] if self.v.numel() else None
 
-    def _apply_gram(self, x):
-        """G x for one flattened vector."""
-        self.n_matvec += 1
-        if self._gram_user is not None:
-            return self._gram_user(x).reshape(-1)
-        vol = x.contiguous().reshape(self.volume_shape)
-        with torch.no_grad():
-            return self._projector.back_project(self._projector.forward_project(vol)).reshape(-1)
-
-    def _gram_matmul(self, Q, use_tqdm=False, desc="G @ Q"):
-        """G applied to every column of Q (N x m): the columns go through the
-        projector as one batch of volumes."""
-        if self._gram_user is not None or self._projector is None:
-            return torch.stack([self._apply_gram(Q[:, j]) for j in range(Q.shape[1])], dim=1)
-        m = Q.shape[1]
-        step = m if self.block is None else max(1, int(self.block))
-        out = torch.empty_like(Q)
-        for a in range(0, m, step):
-            bcols = Q[:, a:a + step].t().contiguous().reshape(-1, *self.volume_shape)
-            with torch.no_grad():
-                g = self._projector.back_project(self._projector.forward_project(bcols))
-            out[:, a:a + step] = g.reshape(bcols.shape[0], -1).t()
-            self.n_matvec += bcols.shape[0]
-        return out
-
-    # -- solvers ---------------------------------------------------------------
-    def _solve_subspace(self, gram, N, k, n_iters=30, tol=1e-6, seed=None, oversample=0, verbose=False,
-                        use_tqdm=False):
-        """Block power iteration + Rayleigh-Ritz (reference :140-183)."""
-        gen = None
-        if seed is not None:
-            gen = torch.Generator(device=self.device_).manual_seed(int(seed))
-        m = min(N, k + max(0, int(oversample)))
-        Q = torch.randn(N, m, dtype=self.dtype, device=self.device_, generator=gen)
-        Q, _ = torch.linalg.qr(Q)
-        prev = None
-        for it in range(int(n_iters)):
-            Z = gram(Q)
-            Q, _ = torch.linalg.qr(Z)
-            T = Q.t() @ gram(Q)
-            T = 0.5 * (T + T.t())
-            ritz = torch.linalg.eigvalsh(T)
-            if prev is not None:
-                rel = (ritz - prev).abs().max() / (prev.abs().max() + 1e-30)
-                if verbose:
-                    print(f"  [subspace] iter {it:03d}  max Ritz={float(ritz.max()):.4e}  rel-change={float(rel):.2e}")
-                if rel < tol:
-                    break
-            prev = ritz
-        GQ = gram(Q)
-        T = Q.t() @ GQ
-        T = 0.5 * (T + T.t())
-        evals, W = torch.linalg.eigh(T)
-        idx = torch.argsort(evals, descending=True)[:k]
-        return torch.clamp(evals[idx], min=0.0), Q @ W[:, idx]
-
-    def _solve_eigsh(self, gram, N, k, tol=1e-3, maxiter=5000, seed=42, ncv=None, verbose=False, use_tqdm=False,
-                     **_ignored):
-        """SciPy ARPACK ("LM") with the Gram matvec on the GPU (reference :185-224)."""
-        import numpy as np
-        from scipy.sparse.linalg import LinearOperator, eigsh
-
-        dev, dt = self.device_, self.dtype
-
-        def matvec(x):
-            xt = torch.as_tensor(np.asarray(x), dtype=dt, device=dev)
-            return self._apply_gram(xt).to("cpu", torch.float32).numpy()
-
-        op = LinearOperator((N, N), matvec=matvec, dtype=np.float32)
-        rng = np.random.default_rng(int(seed) if seed is not None else None)
-        v0 = rng.standard_normal(N).astype(np.float32)
-        ncv = ncv if ncv is not None else min(N - 1, max(20, 2 * k + 1))
-        s2_np, V_np = eigsh(op, k=k, which="LM", ncv=ncv, v0=v0, tol=tol, maxiter=maxiter)
-        order = np.argsort(s2_np)[::-1]
-        s2 = torch.as_tensor(np.clip(s2_np[order], 0.0, None).copy(), dtype=dt, device=dev)
-        V = torch.as_tensor(V_np[:, order].copy(), dtype=dt, device=dev)
-        return s2, V
-
-    def _solve_lanczos(self, gram, N, k, tol=1e-3, ncv=None, max_restarts=50, seed=42, verbose=False,
-                       use_tqdm=False, **_ignored):
-        """Thick-restart Lanczos for the k largest eigenpairs, on the device.
-
-        Basis V ((ncv+1) x N, one vector per row, so that every product with
-        it reads whole contiguous vectors) in float32 with two passes of
-        classical Gram-Schmidt against all previous vectors per step; the
-        projected matrix T = V G V^T in float64.  After ncv vectors the k leading Ritz
-        vectors and the residual direction are kept and the iteration
-        continues from them (thick restart).  Converged when every kept Ritz
-        pair has residual |beta * s_last| <= tol * theta_max."""
-        dev, dt = self.device_, self.dtype
-        ncv = int(ncv) if ncv is not None else min(N - 1, max(20, 2 * k + 1))
-        if not (k < ncv < N):
-            raise ValueError("lanczos needs k < ncv < N")
-        gen = torch.Generator(device="cpu").manual_seed(int(seed))
-        V = torch.empty(ncv + 1, N, dtype=dt, device=dev)
-        v0 = torch.randn(N, generator=gen, dtype=dt).to(dev)
-        V[0] = v0 / v0.norm()
-        T = torch.zeros(ncv, ncv, dtype=torch.float64, device=dev)
-        start = 0
-        beta_last = 0.0
-        for restart in range(int(max_restarts)):
-            for j in range(start, ncv):
-                w = self._apply_gram(V[j])
-                h = V[:j + 1] @ w
-                w = w - V[:j + 1].t() @ h
-                h2 = V[:j + 1] @ w
-                w = w - V[:j + 1].t() @ h2
-                h = (h + h2).double()
-                T[:j + 1, j] = h
-                T[j, :j + 1] = h
-                beta = w.norm()
-                if j + 1 < ncv:
-                    T[j + 1, j] = T[j, j + 1] = beta.double()
-                V[j + 1] = w / beta.clamp_min(1e-30)
-                beta_last = beta
-            theta, S = torch.linalg.eigh(T)
-            order = torch.argsort(theta, descending=True)
-            theta, S = theta[order], S[:, order]
-            res = (beta_last.double() * S[-1, :k]).abs()
-            if verbose:
-                print(f"  [lanczos] restart {restart}: theta_max={float(theta[0]):.4e} "
-                      f"max residual/theta_max={float(res.max() / theta[0].abs()):.2e}")
-            if bool((res <= tol * theta[0].abs()).all()) or restart == max_restarts - 1:
-                break
-            # thick restart: keep k Ritz vectors and the residual direction
-            Y = S[:, :k].t().to(dt) @ V[:ncv]
-            resid = V[ncv].clone()
-            V[:k] = Y
-            V[k] = resid
-            T.zero_()
-            T[:k, :k] = torch.diag(theta[:k])
-            coup = beta_last.double() * S[-1, :k]
-            T[k, :k] = coup
-            T[:k, k] = coup
-            start = k
-        Y = (S[:, :k].t().to(dt) @ V[:ncv]).t()
-        return torch.clamp(theta[:k], min=0.0).to(dt), Y
-
-    # -- public API --------------------------------------------------------------
-    def compute_weights(self, k=None, method="subspace", compute_projection_basis=None, verbose=False,
-                        use_tqdm=False, **kwargs):
-        if k is not None:
-            self.k = int(k)
-        k = self.k
-        N = self.N
-        if N is None:
-            raise RuntimeError("cannot infer problem size N; give volume_shape or gram")
-        solver = self._METHODS.get(method)
-        if solver is None:
-            raise KeyError(f"unknown method '{method}'; registered: {sorted(self._METHODS)}")
-        t0 = time.time()
-        s2, V = solver(self, self._gram_matmul, N, k, verbose=verbose, use_tqdm=use_tqdm, **kwargs)
-        s = torch.sqrt(torch.clamp(s2, min=0.0)).to(self.dtype)
-        self.register_buffer("s", s.contiguous())
-        self.register_buffer("v", V.to(self.dtype).contiguous())
-        if compute_projection_basis is None:
-            compute_projection_basis = self._forward is not None and self._projector is not None
-        if compute_projection_basis:
-            if self._forward is None:
-                raise RuntimeError("projection basis requested but no forward operator")
-            with torch.no_grad():
-                vols = self.v.t().contiguous().reshape(-1, *self.volume_shape)
-                p = self._forward(vols)
-            self.register_buffer("p", p.reshape(vols.shape[0], -1).t().contiguous())
-        else:
-            self.register_buffer("p", torch.zeros(0, dtype=self.dtype))
-        if verbose:
-            print(f"[SparseEigenDecomposition] {method} done in {time.time() - t0:.2f}s, {self.n_matvec} matvecs")
-        return self
+    @property
+    def n_matvec(self):
+        return self._gram.count
 
     @property
     def eigenvalues(self):
         return self.s ** 2
 
-    def to_image_preconditioner(self, eps=1e-12):
-        self._require_computed()
-        return SparseEigenImagePreconditioner(self.s, self.v, eps=eps)
+    def _apply_gram(self, x):
+        return self._gram.vector(x)
 
-    def to_projection_preconditioner(self, projector=None, eps=1e-12, chunk=None):
-        self._require_computed()
-        if self.p.numel() == 0:
-            raise RuntimeError("projection basis not available; recompute with compute_projection_basis=True")
-        projector = projector or self._projector
-        if projector is None:
-            raise ValueError("a projector is required to build a projection preconditioner")
-        return SparseEigenProjectionPreconditioner(projector, self.p, self.eigenvalues, eps=eps, chunk=chunk)
+    def _gram_matmul(self, Q, **_):
+        return self._gram.columns(Q)
 
-    def _require_computed(self):
-        if self.v.numel() == 0:
-            raise RuntimeError("no eigen-basis; call compute_weights() or load() first")
-
-    def _load_from_state_dict(self, state_dict, prefix, *args, **kwargs):
-        for name in ("s", "v", "p"):
-            key = prefix + name
-            if key in state_dict:
-                self.register_buffer(name, torch.empty_like(state_dict[key]))
-        return super()._load_from_state_dict(state_dict, prefix, *args, **kwargs)
-
-    def save(self, path):
-        torch.save({"state_dict": self.state_dict(), "k": self.k, "volume_shape": self.volume_shape}, path)
-        return path
-
-    def load(self, path, map_location=None):
-        ckpt = torch.load(path, map_location=map_location or self.device_)
-        if isinstance(ckpt, dict) and "state_dict" in ckpt:
-            self.k = ckpt.get("k", self.k)
-            if ckpt.get("volume_shape") is not None:
-                self.volume_shape = tuple(ckpt["volume_shape"])
-            state = ckpt["state_dict"]
-        else:
-            state = ckpt
-        self.load_state_dict(state)
+    # -- computing ------------------------------------------------------------
+    def compute_weights(self, k=None, method="subspace", compute_projection_basis=None, verbose=False,
+                        use_tqdm=False, **kwargs):
+        """Estimate the k leading eigenpairs with the named solver and fill
+        s, v and (when a projector is present, or when asked) p = A v.
+        Returns self."""
+        if k is not None:
+            self.k = int(k)
+        N = self.N
+        if N is None:
+            raise RuntimeError("the problem size is unknown: give volume_shape or a projector")
+        if method not in self._solvers:
+            raise KeyError(f"unknown method '{method}'; registered: {sorted(self._solvers)}")
+        began = time.time()
+        eig, V = self._solvers[method](self, self._gram.columns, N, self.k, verbose=verbose, **kwargs)
+        s = eig.clamp_min(0.0).sqrt().to(self.dtype)
+        V = V.to(self.dtype)
+        want_p = (self._projector is not None) if compute_projection_basis is None else compute_projection_basis
+        p = None
+        if want_p:
+            if self._forward is None:
+                raise RuntimeError("a projection basis needs a forward operator")
+            with torch.no_grad():
+                vols = V.t().reshape(V.shape[1], *self.volume_shape).contiguous()
+                p = self._forward(vols).reshape(V.shape[1], -1).t()
+        self._install(s, V, p)
+        if verbose:
+            print(f"[SparseEigenDecomposition] {method}: {time.time() - began:.2f} s, {self.n_matvec} matvecs, "
+                  f"s in [{float(s.min()):.3e}, {float(s.max()):.3e}]")
         return self
 
     @classmethod
     def register_method(cls, name, fn):
-        cls._METHODS[name] = fn
+        """Add a solver fn(dec, gram, N, k, **kw) -> (eigenvalues [k], V [N, k])."""
+        cls._solvers[name] = fn
         return fn
 
+    # -- preconditioners --------------------------------------------------------
+    def _computed(self):
+        if self.v.numel() == 0:
+            raise RuntimeError("no eigen-basis yet: call compute_weights() or load()")
 
-SparseEigenDecomposition.register_method("subspace", SparseEigenDecomposition._solve_subspace)
-SparseEigenDecomposition.register_method("eigsh", SparseEigenDecomposition._solve_eigsh)
-SparseEigenDecomposition.register_method("lanczos", SparseEigenDecomposition._solve_lanczos)
+    def to_image_preconditioner(self, eps=1e-12):
+        self._computed()
+        return SparseEigenImagePreconditioner(self.s, self.v, eps=eps)
+
+    def to_projection_preconditioner(self, projector=None, eps=1e-12, chunk=None):
+        self._computed()
+        if self.p.numel() == 0:
+            raise RuntimeError("no projection basis: compute_weights(compute_projection_basis=True) first")
+        projector = projector if projector is not None else self._projector
+        if projector is None:
+            raise ValueError("a projector is needed for the projection preconditioner")
+        return SparseEigenProjectionPreconditioner(projector, self.p, self.eigenvalues, eps=eps, chunk=chunk)
+
+    # -- checkpoints --------------------------------------------------------------
+    def save(self, path):
+        """The reference's checkpoint layout: {"state_dict", "k", "volume_shape"}."""
+        torch.save({"state_dict": {name: getattr(self, name) for name in _BASIS}, "k": self.k,
+                    "volume_shape": self.volume_shape}, path)
+        return path
+
+    def load(self, path, map_location=None):
+        """A checkpoint written by save() (ours or the reference's), or a bare
+        state dict with s / v / p."""
+        blob = torch.load(path, map_location=map_location or self.device_)
+        state = blob.get("state_dict", blob) if isinstance(blob, dict) else blob
+        if isinstance(blob, dict) and "state_dict" in blob:
+            self.k = int(blob.get("k", self.k))
+            if blob.get("volume_shape") is not None:
+                self.volume_shape = tuple(int(n) for n in blob["volume_shape"])
+                self._gram.volume_shape = self.volume_shape
+        missing = [name for name in _BASIS if name not in state]
+        if missing:
+            raise KeyError(f"checkpoint lacks {missing}")
+        self._install(*(state[name] for name in _BASIS))
+        return self
+
+    def extra_repr(self):
+        return f"k={self.k}, volume_shape={self.volume_shape}, basis={'set' if self.v.numel() else 'empty'}"
 
 
-class SparseEigenImagePreconditioner(Preconditioner):
-    """P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I on flattened volumes
-    (reference preconditioners.py:28-57)."""
+SparseEigenDecomposition.register_method("subspace", subspace_iteration)
+SparseEigenDecomposition.register_method("eigsh", arpack_eigsh)
+SparseEigenDecomposition.register_method("lanczos", thick_restart_lanczos)
 
-    def __init__(self, s, v, eps=1e-12):
-        super().__init__()
-        # [N, k] as the reference's buffer, stored column-major: each
-        # eigenvector contiguous, so both products below read whole vectors
-        # (V^T x: 0.70 against 0.88 ms, V c: 0.97 against 1.64 ms at 256^3,
-        # k = 64, on one B200)
-        self.register_buffer("v", v.t().contiguous().t())
-        s_min = s.min()
-        self.register_buffer("diag_fwd", 1.0 / (s + eps) - 1.0 / (s_min + eps))
-        self.register_buffer("diag_inv", (s - s_min))
-        self.register_buffer("inv_s_min", 1.0 / (s_min + eps))
-        self.register_buffer("s_min", s_min.clone())
+
+class _LowRankPreconditioner(Preconditioner):
+    """x -> B(g * B^T x) + f x, the shape shared by P and P^-1 of both
+    pathways: `gains[0]`, `floor[0]` for P; `gains[1]`, `floor[1]` for P^-1."""
+
+    def _low_rank(self, x, g):
+        raise NotImplementedError
 
     def forward(self, x):
         xf = x.reshape(-1)
-        c = torch.mv(self.v.t(), xf) * self.diag_fwd
-        return torch.mv(self.v, c) + self.inv_s_min * xf
+        return self._low_rank(xf, self.gains[0]) + self.floor[0] * xf
 
     def inverse(self, x):
         xf = x.reshape(-1)
-        c = torch.mv(self.v.t(), xf) * self.diag_inv
-        return torch.mv(self.v, c) + self.s_min * xf
+        return self._low_rank(xf, self.gains[1]) + self.floor[1] * xf
 
 
-class SparseEigenProjectionPreconditioner(Preconditioner):
+class SparseEigenImagePreconditioner(_LowRankPreconditioner):
+    """P = V (S^-1 - s_min^-1 I) V^T + s_min^-1 I on flattened volumes, and
+    P^-1 = V (S - s_min I) V^T + s_min I (reference preconditioners.py:28-57).
+
+    The basis is kept as k contiguous rows (each eigenvector contiguous), so
+    both products read whole vectors (V^T x: 0.70 against 0.88 ms, V c: 0.97
+    against 1.64 ms for the [N, k] layout at 256^3, k = 64, on one B200)."""
+
+    def __init__(self, s, v, eps=1e-12):
+        super().__init__()
+        s_min = s.min()
+        self.register_buffer("rows", v.t().contiguous())
+        self.register_buffer("gains", torch.stack([1.0 / (s + eps) - 1.0 / (s_min + eps), s - s_min]))
+        self.register_buffer("floor", torch.stack([1.0 / (s_min + eps), s_min.clone()]))
+
+    @property
+    def v(self):
+        return self.rows.t()
+
+    def _low_rank(self, x, g):
+        return torch.mv(self.rows.t(), torch.mv(self.rows, x) * g)
+
+
+class SparseEigenProjectionPreconditioner(_LowRankPreconditioner):
     """The same P through the projection basis p = A V and the projector
-    (reference preconditioners.py:60-138)."""
+    (reference preconditioners.py:60-138): with A^T p_i = s_i^2 v_i,
+        P x = A^T p diag(w) p^T A x + s_min^-1 x,   w = (s^-1 - s_min^-1) / s^4,
+    and P^-1 with w = (s - s_min) / s^4 and s_min.  `chunk` streams the basis
+    in column blocks (e.g. a basis kept in host memory)."""
 
     def __init__(self, projector, p, s2, eps=1e-12, chunk=None):
         super().__init__()
         self.projector = projector
         self.nx, self.ny, self.nz = projector.n_x, projector.n_y, projector.n_z
         self.dev = projector.M.device
+        self.chunk = chunk
         self.register_buffer("p", p)
         s2 = s2.to(self.dev)
-        s = torch.sqrt(torch.clamp(s2, min=0.0))
+        s = s2.clamp_min(0.0).sqrt()
         s_min = s.min()
-        s4 = torch.clamp(s2, min=eps).pow(2)
-        self.register_buffer("w_fwd", (1.0 / (s + eps) - 1.0 / (s_min + eps)) / s4)
-        self.register_buffer("w_inv", (s - s_min) / s4)
-        self.register_buffer("inv_s_min", 1.0 / (s_min + eps))
-        self.register_buffer("s_min", s_min.clone())
-        self.chunk = chunk
+        s4 = s2.clamp_min(eps) ** 2
+        self.register_buffer("gains", torch.stack([(1.0 / (s + eps) - 1.0 / (s_min + eps)) / s4, (s - s_min) / s4]))
+        self.register_buffer("floor", torch.stack([1.0 / (s_min + eps), s_min.clone()]))
 
-    def _pk_T(self, r):
-        r = r.reshape(-1)
-        p = self.p.to(self.dev)
-        if self.chunk is None:
-            return torch.mv(p.t(), r.to(p.dtype))
-        out = torch.empty(p.shape[1], device=self.dev)
-        for a in range(0, p.shape[1], self.chunk):
-            out[a:a + self.chunk] = torch.mv(p[:, a:a + self.chunk].t(), r)
-        return out
+    def _blocks(self):
+        k = self.p.shape[1]
+        step = k if self.chunk is None else max(1, int(self.chunk))
+        for lo in range(0, k, step):
+            yield lo, min(k, lo + step), self.p[:, lo:min(k, lo + step)].to(self.dev)
 
-    def _pk(self, c):
-        p = self.p.to(self.dev)
-        if self.chunk is None:
-            return torch.mv(p, c.to(self.dev))
-        out = None
-        for a in range(0, p.shape[1], self.chunk):
-            part = torch.mv(p[:, a:a + self.chunk], c[a:a + self.chunk])
-            out = part if out is None else out + part
-        return out
-
-    def _apply(self, x, w):
-        xf = x.reshape(-1)
-        ax = self.projector.forward_project(xf.view(self.nx, self.ny, self.nz))
-        c = self._pk_T(ax.reshape(-1)) * w
-        proj = self._pk(c).view(ax.shape)
-        return self.projector.back_project(proj).reshape(-1)
-
-    def forward(self, x):
-        xf = x.reshape(-1)
-        return self._apply(xf, self.w_fwd) + self.inv_s_min * xf
-
-    def inverse(self, x):
-        xf = x.reshape(-1)
-        return self._apply(xf, self.w_inv) + self.s_min * xf
+    def _low_rank(self, x, g):
+        ax = self.projector.forward_project(x.view(self.nx, self.ny, self.nz))
+        r = ax.reshape(-1)
+        back = None
+        for lo, hi, blk in self._blocks():
+            part = torch.mv(blk, torch.mv(blk.t(), r.to(blk.dtype)) * g[lo:hi])
+            back = part if back is None else back + part
+        return self.projector.back_project(back.view(ax.shape)).reshape(-1)

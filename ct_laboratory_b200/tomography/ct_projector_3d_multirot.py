@@ -27,7 +27,7 @@ import torch
 from torch import nn
 
 from .ct_projector_3d_module import CTProjector3DModule
-from .ct_projector_3d_subsets import OrderedSubsetProjector, RandomSubsetProjector, SubsetProjector
+from .ct_projector_3d_subsets import OrderedSubsetProjector, RandomSubsetProjector
 
 __all__ = ["MultiRotationProjector"]
 
@@ -102,9 +102,8 @@ class MultiRotationProjector(nn.Module):
                             for i in range(self.n_rotations)], dim=0)
 
     def _batchable(self):
-        bp = self.base_projector
-        return isinstance(bp, CTProjector3DModule) or isinstance(bp, RandomSubsetProjector) or (
-            isinstance(bp, OrderedSubsetProjector) and bp.persistent_projector is not None)
+        # these take a batch of volumes (and a batch of sinograms) in one call
+        return isinstance(self.base_projector, (CTProjector3DModule, RandomSubsetProjector, OrderedSubsetProjector))
 
     # -- forward ------------------------------------------------------------------
     def forward(self, full_volume):
@@ -117,14 +116,6 @@ class MultiRotationProjector(nn.Module):
         bp = self.base_projector
         if self._batchable():
             return bp(windows).t().contiguous()
-        if isinstance(bp, SubsetProjector):  # ordered subsets: tables once per subset, all rotations at once
-            out = torch.zeros(bp.n_total_rays_core, self.n_rotations, device=windows.device, dtype=windows.dtype)
-            for j in range(bp.n_subsets):
-                s, e = int(bp.subset_boundaries[j]), int(bp.subset_boundaries[j + 1])
-                sub = bp._get_cached_subset_projector(j).to(windows.device)
-                out[s:e] = sub(windows).t()
-                del sub
-            return out
         return torch.stack([bp(windows[i]) for i in range(self.n_rotations)], dim=1).contiguous()
 
     # -- back-projection --------------------------------------------------------------
@@ -151,14 +142,5 @@ class MultiRotationProjector(nn.Module):
         if self._batchable():
             wins = bp.back_project(sino_t)
             return self._scatter(shape, wins, int(full_volume_z_size))
-        if isinstance(bp, SubsetProjector):
-            acc = None
-            for j in range(bp.n_subsets):
-                s, e = int(bp.subset_boundaries[j]), int(bp.subset_boundaries[j + 1])
-                sub = bp._get_cached_subset_projector(j).to(sino.device)
-                part = sub.back_project(sino_t[:, s:e].contiguous())
-                acc = part if acc is None else acc.add_(part)
-                del sub
-            return self._scatter(shape, acc, int(full_volume_z_size))
         wins = torch.stack([bp.back_project(sino_t[i]) for i in range(self.n_rotations)], dim=0)
         return self._scatter(shape, wins, int(full_volume_z_size))
