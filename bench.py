@@ -232,11 +232,18 @@ def cpu_baseline(case, target_s=15.0, gpu_view0=None):
         f64 = O.fwd_planesort(case.vol, Mi64, b64, s64, d64, dtype=np.float64)
         a64 = O.back_planesort(y0, Mi64, b64, s64, d64, case.vol.shape, dtype=np.float64)
 
+        # the reference's own float32 arithmetic: the oracle's restatement of
+        # its on-the-fly kernel (ct_projector_3d.cu:902-1012)
+        f32 = O.fwd_planesort(case.vol, case.Mi, case.b, case.src[:pv], case.dst[:pv])
+        a32 = O.back_planesort(y0.astype(np.float32), case.Mi, case.b, case.src[:pv], case.dst[:pv],
+                               case.vol.shape)
+
         def errs(a, ref):
             return {"max_rel": float(np.abs(a - ref).max() / np.abs(ref).max()),
                     "rel_l2": float(np.linalg.norm(a - ref) / np.linalg.norm(ref))}
-        out["fp64_check"] = {"rays": pv, "view": 0, "forward": errs(f_gpu, f64), "adjoint": errs(a_gpu, a64),
-                             "note": "GPU float32 (crossing rule) against the FP64 plane-sort oracle"}
+        out["view_check"] = {"rays": pv, "view": 0,
+                             "vs_reference_f32": {"forward": errs(f_gpu, f32), "adjoint": errs(a_gpu, a32)},
+                             "vs_fp64": {"forward": errs(f_gpu, f64), "adjoint": errs(a_gpu, a64)}}
     return out
 
 
@@ -303,7 +310,7 @@ def run_ours(args, world, rank, local):
                                    voxel_rule=args.voxel_rule, walk=args.walk,
                                    deterministic_adjoint=args.deterministic, block_threads=args.block_threads)
     elif w.name.startswith("static"):
-        # StaticCT ring: under the crossing rule the modules' 16-row columns take the column walk
+        # StaticCT ring: the modules' 16-row columns take the column walk
         proj = w.projector(dev, voxel_rule=args.voxel_rule)
     else:
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
@@ -389,6 +396,11 @@ def run_ours(args, world, rank, local):
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "batched": batched,
                "serving": serving, "map": map_leg,
                "gpu_launches": launches_per_step * args.steps}
+        if cpu is not None and "view_check" in cpu:
+            out["parity"] = dict(cpu["view_check"], bar=1e-5, metric="max |ours - ref| / max |ref|",
+                                 note="view 0 of the benched projector (same kernels, same launch shape) against "
+                                      "the CPU restatement of the reference's float32 on-the-fly kernel and against "
+                                      "its float64 evaluation")
         print(json.dumps(out))
 
 
@@ -670,7 +682,7 @@ def main():
     ap.add_argument("--workload", default="cone256")
     ap.add_argument("--tile-rows", type=int, default=32)
     ap.add_argument("--block-threads", type=int, default=128, help="threads per CTA of the cone-beam launches")
-    ap.add_argument("--voxel-rule", type=int, default=1, help="0 = reference midpoint rule, 1 = crossing rule")
+    ap.add_argument("--voxel-rule", type=int, default=0, help="0 = reference midpoint rule, 1 = crossing rule")
     ap.add_argument("--walk", type=int, default=0, help="0 = auto, 1 = per-lane walk, 2 = column walk")
     ap.add_argument("--deterministic", action="store_true", help="adjoint by the voxel-driven gather")
     ap.add_argument("--views", type=int, default=0,

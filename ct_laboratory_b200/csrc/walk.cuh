@@ -1258,7 +1258,6 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     }
 }
 
-
 // ----------------------------------------------------------------------------
 // Shared x-y walk under the reference's midpoint rule (3-D).
 //
@@ -1267,56 +1266,43 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
 // 982-996).  With a diagonal M^-1 (every off-diagonal entry exactly zero, as
 // standard_image_transform_3d builds it) each index depends on its own axis
 // only: i = rne(m00 (fma(tm, v_x, s_x) - b_x)), and likewise j and k, because
-// the zero products of world_to_index3 add exact zeros.  Each is a chain of
-// monotone roundings of tm, so i(tm), j(tm) and k(tm) are monotone in tm.
+// the zero products of world_to_index3 add exact zeros.
 //
 // Lanes that share their world x-y line (one source, one detector column)
-// share every x- and y-plane parameter and every value of i(tm), j(tm).  The
-// warp derives the merged x-y crossings as in shared_xy_ray, and for each
-// cell [c0, c1] one lane evaluates (i, j) at the cell's midpoint and at
-// lo = c0 + delta and hi = c1 - delta: equal indices at lo, tm and hi prove,
-// by monotonicity, that every midpoint in [lo, hi] rounds to the same (i, j)
-// (a cell whose ends disagree shrinks that side of the interval to tm).  The
-// cell record holds c1, the flat (i, j) offset and [lo, hi].
+// share every x- and y-plane parameter, and for a segment that is a whole x-y
+// cell [c0, c1] they share its midpoint tm and its (i, j).  The warp derives
+// the merged x-y crossings 32 per round as in shared_xy_ray and, one lane per
+// cell, a record: the cell's end, tm, span c1 - c0 and the flat (i, j) offset
+// of the rounded midpoint (or -1 when that is outside the grid).  Each round
+// is then walked in two passes:
 //
-// Each lane then walks its own segments, one per step: the segment ends at
-// the nearer of the cell end and its own next z plane, and the cell cursor
-// and the z plane advance as they are reached (several z planes per cell are
-// fine).  A segment's midpoint tm is formed as the reference forms it; inside
-// the cell's [lo, hi] its (i, j) is the record's and k = k(tm) is evaluated
-// directly; outside (a midpoint within delta of an x-y crossing) the voxel is
-// evaluated in full (midpoint_voxel), so every segment gets the reference's
-// voxel.  The segments just outside the grid whose midpoint rounds onto a face
-// voxel are added from edge_segments, as in traverse<3, ADJ, true>.  The
-// forward sums vol * ((t1 - t0) |v|) in walk order, the reference's terms in
-// the reference's order, so it is bitwise the reference's line integral.
+//  pass 1, all lanes in step, one broadcast record per cell: the whole cell
+//    is one segment in voxel (i, j, k(tm)), k evaluated by each lane with the
+//    reference's arithmetic.  This is the reference's segment for every cell
+//    that holds none of the lane's z planes (and lies inside the lane's own
+//    [t_enter, t_exit]);
+//  pass 2, per lane: each cell that holds one of the lane's z planes, or its
+//    own entry or exit, strictly inside is walked again: its segments (split
+//    at the z planes, clipped to [t_enter, t_exit]) each get the voxel of
+//    their own rounded midpoint (midpoint_voxel), and the whole-cell term
+//    pass 1 added for it, if any, is taken back out.
+//
+// Every segment of the reference inside the grid is thus charged to the
+// reference's voxel with the reference's parameter span; the segments just
+// outside the grid whose midpoint rounds onto a face voxel are added from
+// edge_segments, as in traverse<3, ADJ, true>.  Spans are scaled by |v| once
+// per ray (the forward multiplies its sum, the adjoint its y), and the
+// forward sums in pass order, so results equal the reference's to rounding,
+// not bitwise (the per-lane walk, traverse<3, false, true>, is bitwise).
+// Warps whose lanes do not share their x-y line, or whose M^-1 is not
+// diagonal, run traverse<3, ADJ, true> per lane.
 // ----------------------------------------------------------------------------
 struct __align__(16) MidCell {
-    float t;       // parameter of the crossing that ends the cell
-    int col;       // flat (i, j) offset of the rounded midpoint of the cell (k = 0)
-    float lo, hi;  // every midpoint parameter in [lo, hi] rounds to `col` in x and y
+    float t;     // end of the cell: the crossing that ends it (clipped to the warp's exit when uniform)
+    int col;     // flat (i, j) offset of the cell's rounded midpoint (k = 0); -1 when outside in x or y
+    float tm;    // the cell's midpoint parameter, 0.5 (c0 + c1) as the reference forms it
+    float span;  // c1 - c0
 };
-
-// Margin of the certified interval, 2^-K times the index-space magnitude over
-// |v| of the crossing axis (a few times the rounding noise of a plane
-// crossing); the certificate, not the margin, makes the interval exact.
-#ifndef CTLAB_MID_MARGIN_LOG2
-#define CTLAB_MID_MARGIN_LOG2 22
-#endif
-
-// (i, j) offset of the rounded world midpoint at parameter tm along a
-// diagonal affine; ok = inside the grid in x and y.
-struct XYMidLine {
-    float sx, sy, vx, vy, bx, by, mx, my;
-    int nx, ny, stx, sty;
-};
-
-__device__ __forceinline__ int xy_mid_offset(const XYMidLine& L, float tm, bool& ok) {
-    const int i = rne_int(__fmul_rn(L.mx, __fsub_rn(__fmaf_rn(tm, L.vx, L.sx), L.bx)));
-    const int j = rne_int(__fmul_rn(L.my, __fsub_rn(__fmaf_rn(tm, L.vy, L.sy), L.by)));
-    ok = (unsigned)i < (unsigned)L.nx && (unsigned)j < (unsigned)L.ny;
-    return i * L.stx + j * L.sty;
-}
 
 __device__ __forceinline__ bool affine_is_diagonal(const Affine3& A) {
     return A.m[1] == 0.f && A.m[2] == 0.f && A.m[3] == 0.f && A.m[5] == 0.f && A.m[6] == 0.f && A.m[7] == 0.f;
@@ -1337,7 +1323,17 @@ __device__ __forceinline__ void edge_planes(const LaneRay& R, float t, const Gri
     }
 }
 
-// Segments walked per step of the midpoint walk (forward: gathers in flight).
+// Number of the W sorted values v[0..W-1] that are <= key (a branch-free
+// binary search over this lane's own key; v in shared memory).
+template <int W>
+__device__ __forceinline__ int count_le(const float* v, float key) {
+    int c = 0;
+#pragma unroll
+    for (int step = W / 2; step > 0; step >>= 1) c += v[c + step - 1] <= key ? step : 0;
+    return c + (v[c] <= key ? 1 : 0);
+}
+
+// Cells per pass-1 step (forward: gathers in flight per lane).
 #ifndef CTLAB_MID_GROUP_FWD
 #define CTLAB_MID_GROUP_FWD 8
 #endif
@@ -1442,40 +1438,17 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         psy = va1 > 0.f ? 1.f : -1.f;
         pny = (float)slab_at(t_start, s1, va1, i1, G.n[1]) + 0.5f * psy;
     }
-    XYMidLine L;
-    L.sx = sx;
-    L.sy = sy;
-    L.vx = __fsub_rn(dx, sx);
-    L.vy = __fsub_rn(dy, sy);
-    L.bx = A.b[0];
-    L.by = A.b[1];
-    L.mx = A.m[0];
-    L.my = A.m[4];
-    L.nx = G.n[0];
-    L.ny = G.n[1];
-    L.stx = G.stride[0];
-    L.sty = G.stride[1];
-    // certification margin: the smaller of the x and y crossing noise
-    // estimates (index-space magnitude 2^-K / |v|), in parameter units
-    float delta = kInf;
-    {
-        const float kM = 1.f / (float)(1 << CTLAB_MID_MARGIN_LOG2);
-        const float magx = fabsf(A.m[0]) * (fabsf(sx) + fabsf(dx) + fabsf(A.b[0])) + fabsf(s0) +
-                           fabsf(__fadd_rn(s0, va0)) + (float)G.n[0];
-        const float magy = fabsf(A.m[4]) * (fabsf(sy) + fabsf(dy) + fabsf(A.b[1])) + fabsf(s1) +
-                           fabsf(__fadd_rn(s1, va1)) + (float)G.n[1];
-        if (i0 != 0.f) delta = fminf(delta, kM * magx * fabsf(i0));
-        if (i1 != 0.f) delta = fminf(delta, kM * magy * fabsf(i1));
-    }
+    // (i, j) of a world midpoint on the shared x-y line (diagonal M^-1)
+    const float lvx = __fsub_rn(dx, sx), lvy = __fsub_rn(dy, sy);
 
-    // ---- per-lane state: z plane, segment start, constants of k(tm) -------
-    float t_cur = 0.f, t_end = 0.f, tnz = kInf, pnz = 0.f, psz = 0.f;
+    // ---- per-lane state: own entry / exit, next z plane, k(tm) constants --
+    float t_enter = 0.f, t_exit = 0.f, tnz = kInf, pnz = 0.f, psz = 0.f;
     if (R.live) {
-        t_cur = R.t_enter;
-        t_end = R.t_exit;
+        t_enter = R.t_enter;
+        t_exit = R.t_exit;
         if (R.inv[2] != 0.f) {
             psz = R.va[2] > 0.f ? 1.f : -1.f;
-            pnz = (float)slab_at(t_cur, R.s[2], R.va[2], R.inv[2], G.n[2]) + 0.5f * psz;
+            pnz = (float)slab_at(t_enter, R.s[2], R.va[2], R.inv[2], G.n[2]) + 0.5f * psz;
             tnz = plane_t(pnz, R.s[2], R.inv[2]);
         }
     }
@@ -1483,6 +1456,11 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
     const float zs0 = sw[2], zv = vw[2], zb = A.b[2], zm = A.m[8];
     const unsigned nz = (unsigned)G.n[2];
     const float len = R.ray_len;
+    // Without the uniform walk's clipping of the cell ends, pass 2 also
+    // walks the cell holding a lane's own entry (when it enters after the
+    // first cell's start, t_start) and the one holding its exit (for every
+    // live lane: the last cell may end past even the latest exit).
+    bool pend_enter = R.live && t_enter > t_start, pend_exit = R.live;
 
     const float* vol[NB];
     float* vout[NB];
@@ -1496,30 +1474,33 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         yl[j] = __fmul_rn(y[j], len);  // adjoint: y * |v|, times each parameter span
     }
     const uint64_t pol = l2_policy_keep();
+    // one segment of voxel v and parameter span w into every volume
+    auto charge = [&](int v, float w, bool use) {
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            if constexpr (ADJ) {
+                red_add_if(vout[j] + (unsigned)v, __fmul_rn(yl[j], w), use && (NB == 1 || j < nb));
+            } else {
+                if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)v, pol), w, acc[j]);
+            }
+        }
+    };
+    // k of the rounded midpoint at tm (this lane's z line)
+    auto k_at = [&](float tm) { return rne_int(__fmul_rn(zm, __fsub_rn(__fmaf_rn(tm, zv, zs0), zb))); };
 
-    // ---- segments just before the entry (ascending, as the reference sums)
+    // ---- segments just before the entry (spans: edge_segments with |v| = 1)
     if (R.live) {
         float p0[3], ps[3], el[kEdge];
         int ev[kEdge];
-        edge_planes<-1>(R, t_cur, G, p0, ps);
-        const int ne = edge_segments<3, -1>(A, sw, vw, R.s, R.inv, ps, p0, t_cur, len, G, ev, el);
+        edge_planes<-1>(R, t_enter, G, p0, ps);
+        const int ne = edge_segments<3, -1>(A, sw, vw, R.s, R.inv, ps, p0, t_enter, 1.f, G, ev, el);
 #pragma unroll
-        for (int k = kEdge - 1; k >= 0; --k) {
-            const bool use = k < ne && el[k] > 0.f;
-#pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                if constexpr (ADJ) {
-                    red_add_if(vout[j] + (unsigned)ev[k], __fmul_rn(y[j], el[k]), use && (NB == 1 || j < nb));
-                } else {
-                    if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)ev[k], pol), el[k], acc[j]);
-                }
-            }
-        }
+        for (int k = kEdge - 1; k >= 0; --k) charge(ev[k], el[k], k < ne && el[k] > 0.f);
     }
 
     const float fl = (float)lane;
     const int max_rounds = (G.n[0] + G.n[1] + 2) / W + 2;
-    const int max_steps = W + G.n[2] + 2;  // cells of a round plus the z planes crossed in it
+    const int max_steps = W + G.n[2] + 4;  // pass-2 cells of a round: at most one per z plane, entry and exit
     constexpr int kNG = ADJ ? CTLAB_MID_GROUP_ADJ : (CTLAB_MID_GROUP_FWD / NB > 0 ? CTLAB_MID_GROUP_FWD / NB : 1);
     const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
     float carry = t_start;  // start of the round's first cell
@@ -1534,7 +1515,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
             const int kx = warp_rank<true, W>(tx, ty);
             const int rx = lane + ky;
             const int ry = lane + kx;
-            if (UNI) {
+            if (UNI) {  // cell ends past the common exit are the exit
                 tx = fminf(tx, t_stop);
                 ty = fminf(ty, t_stop);
             }
@@ -1543,69 +1524,41 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
             const int n_x = __popc(__ballot_sync(kFullMask, rx < W) & gmask);
             __syncwarp();
             const float c1 = raw[lane];
-            const float c0 = lane == 0 ? carry : raw[lane - 1];
+            const float r0 = carry;
+            const float c0 = lane == 0 ? r0 : raw[lane - 1];
             const int n_in = __popc(__ballot_sync(kFullMask, c1 < t_stop) & gmask);
             const int n_cells = (W == 16 && fin) ? 0 : min(n_in + 1, W);
             carry = __shfl_sync(kFullMask, c1, (wlane & (32 - W)) + W - 1);
-            // the record of this lane's cell
-            {
+            {  // the record of this lane's cell
                 const float tm = __fmul_rn(0.5f, __fadd_rn(c0, c1));
-                bool okm, okl, okh;
-                const int col = xy_mid_offset(L, tm, okm);
-                const float d = fmaxf(delta, c1 * (1.f / 2097152.f));
-                float lo = fminf(__fadd_rn(c0, d), tm), hi = fmaxf(__fsub_rn(c1, d), tm);
-                if (xy_mid_offset(L, lo, okl) != col || okl != okm) lo = tm;
-                if (xy_mid_offset(L, hi, okh) != col || okh != okm) hi = tm;
-                if (!okm) {  // midpoint outside the grid in x or y: every segment takes the full evaluation
-                    lo = kInf;
-                    hi = -kInf;
-                }
-                rec[lane] = MidCell{c1, col, lo, hi};
+                const int i = rne_int(__fmul_rn(A.m[0], __fsub_rn(__fmaf_rn(tm, lvx, sx), A.b[0])));
+                const int j = rne_int(__fmul_rn(A.m[4], __fsub_rn(__fmaf_rn(tm, lvy, sy), A.b[1])));
+                const bool in = (unsigned)i < (unsigned)G.n[0] && (unsigned)j < (unsigned)G.n[1];
+                rec[lane] = MidCell{c1, in ? i * G.stride[0] + j * G.stride[1] : -1, tm, __fsub_rn(c1, c0)};
             }
             __syncwarp();
-            int q = 0;  // this lane's cell
+            // ---- pass 1: whole cells, in step -------------------------------
+            float p0 = r0;  // start of the step's first cell
 #pragma unroll 1
-            for (int st = 0; st < max_steps && __any_sync(kFullMask, q < n_cells); st += kNG) {
+            for (int q = 0; q < n_cells; q += kNG) {
                 int vq[kNG];
-                float lq[kNG];
+                float wq[kNG];
                 bool uq[kNG];
 #pragma unroll
                 for (int u = 0; u < kNG; ++u) {
-                    const bool active = q < n_cells;
-                    const MidCell c = rec[q < W ? q : W - 1];
-                    const float te = UNI ? c.t : fminf(c.t, t_end);
-                    const float t1 = fminf(tnz, te);
-                    const float span = __fsub_rn(t1, t_cur);
-                    const bool pos = active && span > 0.f;
-                    const float tm = __fmul_rn(0.5f, __fadd_rn(t_cur, t1));
-                    const int k = rne_int(__fmul_rn(zm, __fsub_rn(__fmaf_rn(tm, zv, zs0), zb)));
-                    const bool in_xy = tm >= c.lo && tm <= c.hi;
-                    int v = c.col + k;
-                    bool use = pos && in_xy && (unsigned)k < nz;
-                    if (pos && !in_xy) {  // midpoint near an x-y crossing: the full evaluation
-                        v = midpoint_voxel<3>(A, sw, vw, t_cur, t1, G);
-                        use = v >= 0;
-                    }
-                    vq[u] = use ? v : 0;
+                    const MidCell c = rec[min(q + u, W - 1)];
+                    const int k = k_at(c.tm);
+                    bool use = q + u < n_cells && c.col >= 0 && (unsigned)k < nz;
+                    if (!UNI) use = use && p0 >= t_enter && c.t <= t_exit;
+                    vq[u] = use ? c.col + k : 0;
+                    wq[u] = c.span;
                     uq[u] = use;
-                    lq[u] = ADJ ? span : __fmul_rn(span, len);
-                    if (active) {
-                        const bool zstep = tnz <= te, cstep = te <= tnz;
-                        if (zstep) {
-                            pnz += psz;
-                            tnz = plane_t(pnz, s2, i2);
-                        }
-                        q += cstep ? 1 : 0;
-                        t_cur = UNI ? t1 : fmaxf(t_cur, t1);
-                    }
-                    if constexpr (ADJ) {
-#pragma unroll
-                        for (int j = 0; j < NB; ++j)
-                            red_add_if(vout[j] + (unsigned)vq[u], __fmul_rn(yl[j], lq[u]),
-                                       uq[u] && (NB == 1 || j < nb));
-                    }
+                    p0 = c.t;
                 }
-                if constexpr (!ADJ) {
+                if constexpr (ADJ) {
+#pragma unroll
+                    for (int u = 0; u < kNG; ++u) charge(vq[u], wq[u], uq[u]);
+                } else {
                     float vv[NB][kNG];
 #pragma unroll
                     for (int j = 0; j < NB; ++j)
@@ -1614,7 +1567,53 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
 #pragma unroll
                     for (int j = 0; j < NB; ++j)
 #pragma unroll
-                        for (int u = 0; u < kNG; ++u) acc[j] = uq[u] ? __fmaf_rn(vv[j][u], lq[u], acc[j]) : acc[j];
+                        for (int u = 0; u < kNG; ++u) acc[j] = uq[u] ? __fmaf_rn(vv[j][u], wq[u], acc[j]) : acc[j];
+                }
+            }
+            // ---- pass 2: this lane's cells with a z plane, entry or exit inside
+            // (the loop and its vote are taken by the whole warp: with W = 16
+            // a finished group has no cells, an empty range and no work)
+            {
+                const float r1 = n_cells > 0 ? raw[n_cells - 1] : -kInf;  // end of the round's last cell
+#pragma unroll 1
+                for (int it = 0; it < max_steps; ++it) {
+                    float bp = tnz < t_exit ? tnz : kInf;
+                    if (!UNI) {
+                        bp = pend_enter ? fminf(bp, t_enter) : bp;
+                        bp = pend_exit ? fminf(bp, t_exit) : bp;
+                    }
+                    const bool work = bp < r1;
+                    if (!__any_sync(kFullMask, work)) break;
+                    if (work) {
+                        const int q = count_le<W>(raw, bp);  // the cell holding bp: c0 <= bp < c1
+                        const float e0 = q == 0 ? r0 : raw[q - 1], e1 = raw[q];
+                        const float lo = UNI ? e0 : fmaxf(e0, t_enter), hi = UNI ? e1 : fminf(e1, t_exit);
+                        // the cell's segments: split at the z planes inside, the last one ending at hi
+                        float t = lo;
+#pragma unroll 1
+                        for (int zs = 0; zs < max_steps; ++zs) {
+                            const bool zin = tnz < hi;
+                            const float e = zin ? tnz : hi;
+                            if (e > t) {
+                                const int v = midpoint_voxel<3>(A, sw, vw, t, e, G);
+                                charge(v, __fsub_rn(e, t), v >= 0);
+                                t = e;
+                            }
+                            if (!zin) break;
+                            pnz += psz;
+                            tnz = plane_t(pnz, s2, i2);
+                        }
+                        // take back pass 1's whole-cell term of this cell
+                        const MidCell c = rec[q];
+                        const int k = k_at(c.tm);
+                        bool full = c.col >= 0 && (unsigned)k < nz;
+                        if (!UNI) full = full && e0 >= t_enter && e1 <= t_exit;
+                        charge(full ? c.col + k : 0, -c.span, full);
+                        if (!UNI) {
+                            pend_enter = pend_enter && !(t_enter < e1);
+                            pend_exit = pend_exit && !(t_exit <= e1);
+                        }
+                    }
                 }
             }
             if constexpr (W == 32) {
@@ -1642,26 +1641,16 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
     if (R.live) {
         float p0[3], ps[3], el[kEdge];
         int ev[kEdge];
-        edge_planes<1>(R, t_end, G, p0, ps);
-        const int ne = edge_segments<3, 1>(A, sw, vw, R.s, R.inv, ps, p0, t_end, len, G, ev, el);
+        edge_planes<1>(R, t_exit, G, p0, ps);
+        const int ne = edge_segments<3, 1>(A, sw, vw, R.s, R.inv, ps, p0, t_exit, 1.f, G, ev, el);
 #pragma unroll
-        for (int k = 0; k < kEdge; ++k) {
-            const bool use = k < ne && el[k] > 0.f;
-#pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                if constexpr (ADJ) {
-                    red_add_if(vout[j] + (unsigned)ev[k], __fmul_rn(y[j], el[k]), use && (NB == 1 || j < nb));
-                } else {
-                    if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)ev[k], pol), el[k], acc[j]);
-                }
-            }
-        }
+        for (int k = 0; k < kEdge; ++k) charge(ev[k], el[k], k < ne && el[k] > 0.f);
     }
     if constexpr (!ADJ) {
         if (r >= 0) {
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, acc[j]);
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(acc[j], len));
         }
     }
 }

@@ -7,13 +7,18 @@ oracle, on geometries built to exercise each branch:
   a column no longer share their x-y line and every warp falls back to the
   per-lane walk inside the same launch;
 * a tall detector close to the source: its outer rows are steeper in z than
-  the column walk admits (|v_z| > 0.75 |v_xy|), so those warps fall back
-  while the central rows' warps walk the column, in one launch.
+  the crossing rule's column walk admits (|v_z| > 0.75 |v_xy|), so under
+  that rule those warps fall back while the central rows' warps walk the
+  column, in one launch; the midpoint rule's column walk takes several z
+  planes per cell and walks every warp of it.
 
-In every case the detector-row tiling (column walk where it applies) gives
-the forward bitwise equal to the flat launch (per-lane walk everywhere), the
-adjoint equal up to the order of the float atomic additions (1e-6 here), and
-both agree with the oracle's plane-sort walk within the projector tolerance
+Under the crossing rule the detector-row tiling (column walk where it
+applies) gives the forward bitwise equal to the flat launch (per-lane walk
+everywhere).  Under the midpoint rule the column walk needs a diagonal M^-1
+(the rotated and tilted affines walk per lane, bitwise as well) and, where it
+runs, sums the same segments in another order: equal to 1e-6.  Adjoints are
+equal up to the order of the float atomic additions (1e-6 here), and both
+walks agree with the oracle's plane-sort walk within the projector tolerance
 1e-5 under the midpoint rule, where that oracle is the reference's own rule.
 """
 import math
@@ -73,7 +78,10 @@ def test_column_walk_branches_match_per_lane_walk(kind, rule):
     args = (T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]))
     f_col = _C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=col)
     f_flat = _C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=flat)
-    assert torch.equal(f_col, f_flat)
+    if rule == 1 or kind != "steep":
+        assert torch.equal(f_col, f_flat)
+    else:  # the midpoint column walk: the same segments summed in another order
+        assert rel_err(f_col.cpu().numpy(), f_flat.cpu().numpy()) < 1e-6
     dims = [int(v) for v in c["n"]]
     b_col = _C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=col)
     b_flat = _C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=flat)

@@ -241,9 +241,11 @@ def test_invert_matrix_exact_for_diagonal():
 @pytest.mark.parametrize("rule", [0, 1])
 def test_voxel_rules_and_column_walk(rule):
     """Both voxel rules, flat (per-lane walk) and detector-row tiling (column
-    walk): the two walks give bitwise equal outputs; the midpoint rule agrees
-    with the restated reference kernel, the crossing rule with the FP64
-    oracle's segment assignment."""
+    walk): the two walks give equal outputs (crossing rule bitwise; midpoint
+    rule to summation order, the column walk adding whole cells first and the
+    cells holding a z plane after); the midpoint rule agrees with the
+    restated reference kernel, the crossing rule with the FP64 oracle's
+    segment assignment."""
     from ct_laboratory_b200 import _native as N
     C = _c()
     c = cone_case(seed=7)
@@ -253,7 +255,10 @@ def test_voxel_rules_and_column_walk(rule):
     args = (T(c["src"]), T(c["dst"]), T(c["Minv"]), T(c["b"]))
     f_col = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=col)
     f_flat = C.forward_project_3d_on_the_fly_cuda(T(c["vol"]), *args, tiling=flat)
-    assert torch.equal(f_col, f_flat)
+    if rule == 1:
+        assert torch.equal(f_col, f_flat)
+    else:
+        assert rel_err(f_col.cpu().numpy(), f_flat.cpu().numpy()) < 1e-6
     dims = [int(v) for v in c["dims"]]
     b_col = C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=col)
     b_flat = C.back_project_3d_on_the_fly_cuda(T(c["y"]), *args, *dims, tiling=flat)

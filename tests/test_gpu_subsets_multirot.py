@@ -87,7 +87,10 @@ def test_random_subset_is_the_core_on_those_rays():
     idx = torch.randperm(core.src.shape[0])[:500]
     assert torch.equal(rsp.current_indices, idx)
     x = rnd(24, 20, 16, seed=5)
-    assert torch.equal(rsp(x), core(x)[idx.to(DEV)])
+    # the subset has no detector layout (flat launch, per-lane walk) while the
+    # core takes the column walk: the same segments and voxels, summed in
+    # another order
+    assert rel_err(rsp(x).cpu().numpy(), core(x)[idx.to(DEV)].cpu().numpy()) < TOL
     rsp.randomize_projector(seed=8)
     assert not torch.equal(rsp.current_indices, idx)
 
