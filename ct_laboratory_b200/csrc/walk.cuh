@@ -904,6 +904,41 @@ __device__ __forceinline__ int warp_rank(float sorted, float key) {
     return c + ((INCLUSIVE ? v <= key : v < key) ? 1 : 0);
 }
 
+// Merged positions of a round's x and y crossings: lane l holds the l-th next
+// x crossing tx and the l-th next y crossing ty (each non-decreasing over the
+// lanes of its group of W); on equal parameters the x crossing comes first:
+//     ky = #{k : ty_k < tx},   kx = #{k : tx_k <= ty}.
+// With CTLAB_XY_RANK_EST (32-lane groups crossing both axes) the counts are
+// estimated from the plane coordinate each parameter falls at (the y index
+// reached at tx, the x index reached at ty) and checked against the two
+// neighbouring lanes: a count is exact when the lane below is on the near
+// side and the lane at the count on the far side.  Any miss in the warp: the
+// binary search (warp_rank).  16-lane groups always search (two steps
+// shorter there, and measured faster than the estimate).  `both` must be
+// warp-uniform.
+template <int W>
+__device__ __forceinline__ void xy_merge_ranks(float tx, float ty, bool both, float s0, float s1, float va0,
+                                               float va1, float pnx, float pny, float psx, float psy, int& kx,
+                                               int& ky) {
+#if CTLAB_XY_RANK_EST
+    if (W == 32 && both) {
+        const float by = psy * __fmaf_rn(tx, va1, __fsub_rn(s1, pny));
+        const float bx = psx * __fmaf_rn(ty, va0, __fsub_rn(s0, pnx));
+        ky = min(max(__float2int_ru(by), 0), W);
+        kx = min(max(__float2int_rd(bx) + 1, 0), W);
+        const float ylo = __shfl_sync(kFullMask, ty, max(ky - 1, 0), W);
+        const float yhi = __shfl_sync(kFullMask, ty, min(ky, W - 1), W);
+        const float xlo = __shfl_sync(kFullMask, tx, max(kx - 1, 0), W);
+        const float xhi = __shfl_sync(kFullMask, tx, min(kx, W - 1), W);
+        const bool ok = (ky == 0 || ylo < tx) && (ky == W || !(yhi < tx)) && (kx == 0 || xlo <= ty) &&
+                        (kx == W || !(xhi <= ty));
+        if (__all_sync(kFullMask, ok)) return;
+    }
+#endif
+    ky = warp_rank<false, W>(ty, tx);
+    kx = warp_rank<true, W>(tx, ty);
+}
+
 // Per-lane z state of the shared x-y walk.
 struct ZWalk {
     float t_cur, t_end, len, tnz, pnz, psz, s2, i2;
@@ -1150,40 +1185,9 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
             // coordinates are exact: |p| < 2^17 in steps of 1)
             float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
             float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
-            // merged positions; on equal parameters the x crossing comes first.
-            // ky = #{k : ty_k < tx}, kx = #{k : tx_k <= ty}, both sequences
-            // non-decreasing over the lanes.
+            // merged positions (x first on equal parameters)
             int ky, kx;
-#if CTLAB_XY_RANK_EST
-            // Estimated from the plane coordinate each parameter falls at
-            // (the y index reached at tx, the x index reached at ty) and
-            // checked against the two neighbouring lanes: the count is exact
-            // when the lane below is on the near side and the lane at the
-            // count on the far side.  Any miss in the warp: the binary search.
-            bool est_ok = false;
-            // (32-lane groups only: a 16-lane binary search is two steps shorter
-            // and measured faster than the estimate there)
-            if (W == 32 && i0 != 0.f && i1 != 0.f) {  // warp-uniform (one x-y line per warp)
-                const float by = psy * __fmaf_rn(tx, va1, __fsub_rn(s1, pny));
-                const float bx = psx * __fmaf_rn(ty, va0, __fsub_rn(s0, pnx));
-                ky = min(max(__float2int_ru(by), 0), W);
-                kx = min(max(__float2int_rd(bx) + 1, 0), W);
-                const float ylo = __shfl_sync(kFullMask, ty, max(ky - 1, 0), W);
-                const float yhi = __shfl_sync(kFullMask, ty, min(ky, W - 1), W);
-                const float xlo = __shfl_sync(kFullMask, tx, max(kx - 1, 0), W);
-                const float xhi = __shfl_sync(kFullMask, tx, min(kx, W - 1), W);
-                const bool ok = (ky == 0 || ylo < tx) && (ky == W || !(yhi < tx)) && (kx == 0 || xlo <= ty) &&
-                                (kx == W || !(xhi <= ty));
-                est_ok = __all_sync(kFullMask, ok);
-            }
-            if (!est_ok) {
-                ky = warp_rank<false, W>(ty, tx);
-                kx = warp_rank<true, W>(tx, ty);
-            }
-#else
-            ky = warp_rank<false, W>(ty, tx);
-            kx = warp_rank<true, W>(tx, ty);
-#endif
+            xy_merge_ranks<W>(tx, ty, i0 != 0.f && i1 != 0.f, s0, s1, va0, va1, pnx, pny, psx, psy, kx, ky);
             const int rx = lane + ky;
             const int ry = lane + kx;
             if (UNI) {  // cell ends past the common exit are the exit
@@ -1511,8 +1515,8 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         for (int round = 0; round < max_rounds; ++round) {
             float tx = i0 != 0.f ? plane_t(__fmaf_rn(fl, psx, pnx), s0, i0) : kInf;
             float ty = i1 != 0.f ? plane_t(__fmaf_rn(fl, psy, pny), s1, i1) : kInf;
-            const int ky = warp_rank<false, W>(ty, tx);
-            const int kx = warp_rank<true, W>(tx, ty);
+            int ky, kx;
+            xy_merge_ranks<W>(tx, ty, i0 != 0.f && i1 != 0.f, s0, s1, va0, va1, pnx, pny, psx, psy, kx, ky);
             const int rx = lane + ky;
             const int ry = lane + kx;
             if (UNI) {  // cell ends past the common exit are the exit
