@@ -1506,6 +1506,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
     const int max_rounds = (G.n[0] + G.n[1] + 2) / W + 2;
     const int max_steps = W + G.n[2] + 4;  // pass-2 cells of a round: at most one per z plane, entry and exit
     constexpr int kNG = ADJ ? CTLAB_MID_GROUP_ADJ : (CTLAB_MID_GROUP_FWD / NB > 0 ? CTLAB_MID_GROUP_FWD / NB : 1);
+    static_assert(W % kNG == 0, "pass-1 steps must tile the round's cells");
     const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
     float carry = t_start;  // start of the round's first cell
     auto rounds = [&](auto uni_tag) {
@@ -1537,7 +1538,8 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
                 const float tm = __fmul_rn(0.5f, __fadd_rn(c0, c1));
                 const int i = rne_int(__fmul_rn(A.m[0], __fsub_rn(__fmaf_rn(tm, lvx, sx), A.b[0])));
                 const int j = rne_int(__fmul_rn(A.m[4], __fsub_rn(__fmaf_rn(tm, lvy, sy), A.b[1])));
-                const bool in = (unsigned)i < (unsigned)G.n[0] && (unsigned)j < (unsigned)G.n[1];
+                // (cells past the round's last walk nothing: col -1 for them too)
+                const bool in = (unsigned)i < (unsigned)G.n[0] && (unsigned)j < (unsigned)G.n[1] && lane < n_cells;
                 rec[lane] = MidCell{c1, in ? i * G.stride[0] + j * G.stride[1] : -1, tm, __fsub_rn(c1, c0)};
             }
             __syncwarp();
@@ -1550,9 +1552,9 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
                 bool uq[kNG];
 #pragma unroll
                 for (int u = 0; u < kNG; ++u) {
-                    const MidCell c = rec[min(q + u, W - 1)];
+                    const MidCell c = rec[q + u];  // q + u < W: kNG divides W
                     const int k = k_at(c.tm);
-                    bool use = q + u < n_cells && c.col >= 0 && (unsigned)k < nz;
+                    bool use = c.col >= 0 && (unsigned)k < nz;
                     if (!UNI) use = use && p0 >= t_enter && c.t <= t_exit;
                     vq[u] = use ? c.col + k : 0;
                     wq[u] = c.span;
