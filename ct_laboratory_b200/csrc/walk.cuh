@@ -1557,7 +1557,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
                     bool use = c.col >= 0 && (unsigned)k < nz;
                     if (!UNI) use = use && p0 >= t_enter && c.t <= t_exit;
                     vq[u] = use ? c.col + k : 0;
-                    wq[u] = c.span;
+                    wq[u] = use ? c.span : 0.f;  // (an unused cell's span may be inf - inf)
                     uq[u] = use;
                     p0 = c.t;
                 }
