@@ -450,7 +450,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 // Device address of g_noalloc_scratch per device.  In host code the array's
 // name is a host-side stand-in, not a device address, so the address is
 // looked up with cudaGetSymbolAddress, once per device with that device
-// current (the first call on each device), and cached.
+// current (the first call on each device), and cached by device ordinal.
+// The cache assumes each device's primary context (the one the runtime API
+// and torch use): a caller that pushes other driver-API contexts of the same
+// device would be handed the primary context's address.
 constexpr int kNoAllocMaxDevices = 64;
 static std::atomic<void*> g_noalloc_addr[kNoAllocMaxDevices];
 

@@ -3,8 +3,8 @@
     python oracle/build_ref.py            # needs the reference checkout
 
 Builds src/bindings.cpp, src/ct_projector_2d.cu and src/ct_projector_3d.cu
-from the read-only reference checkout ($CTLAB_REFERENCE, default
-/root/reference) into oracle/_ref/ctlab_ref_C*.so as a torch extension named
+from the read-only reference checkout ($CTLAB_REFERENCE, else the checkout
+beside this repository: oracle/reference_path.py) into oracle/_ref/ctlab_ref_C*.so as a torch extension named
 ``ctlab_ref_C`` (the reference's ``ct_laboratory._C`` under another name),
 with the flags of its setup.py (-O2) and the sm_100 target of its benchmark
 image (benchmark/Dockerfile:11, TORCH_CUDA_ARCH_LIST=10.0).  No reference
@@ -22,7 +22,6 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("CTLAB_REFERENCE", "/root/reference")
 
 
 def built_path():
@@ -32,6 +31,11 @@ def built_path():
 
 def build(verbose=True):
     from torch.utils.cpp_extension import load
+    try:
+        from oracle.reference_path import reference_root
+    except ImportError:  # run as a script from oracle/
+        from reference_path import reference_root
+    REF = reference_root(required=True)
     src = [os.path.join(REF, "src", f) for f in ("bindings.cpp", "ct_projector_2d.cu", "ct_projector_3d.cu")]
     missing = [s for s in src if not os.path.exists(s)]
     if missing:

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Run in a container that has the reference checkout (read-only) at
-``$CTLAB_REFERENCE`` (default ``/root/reference``)::
+``$CTLAB_REFERENCE`` (else the checkout beside this repository)::
 
     python tests/golden/make_golden.py
 
@@ -37,7 +37,10 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("CTLAB_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.reference_path import reference_root  # noqa: E402
+
+REF = reference_root(required=True)
 
 
 def load_reference():

@@ -20,7 +20,10 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("CTLAB_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.reference_path import reference_root  # noqa: E402
+
+REF = reference_root(required=True)
 
 SHAPE = (16, 16, 8)
 VOXEL = 0.8

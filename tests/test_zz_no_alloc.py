@@ -97,6 +97,36 @@ def test_noalloc_entry_rejects_more_scans_than_its_scratch_holds():
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     rc = N.lib.ctlab_project_batched_noalloc(arr, 65, 0, 0, 256, 0, stream)
     assert rc == 1 and b"at most 64 scans" in N.lib.ctlab_last_error()
-    # the full 64 still run
-    assert N.lib.ctlab_project_batched_noalloc(arr, 64, 0, 0, 256, 0, stream) == 0, N.lib.ctlab_last_error()
+
+
+
+def test_noalloc_entry_at_its_limit_of_64_scans():
+    """64 scans (the most the fixed array holds), each with its own inputs
+    and NaN-filled outputs, against the planned batch of the same 64 scans:
+    a bad table entry or a work counter that stopped early would leave one
+    of them wrong or NaN."""
+    from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.batched import ScanBatch
+    p = _projectors_2d()[0]
+    batch = ScanBatch([p] * 64)
+    img_out = [torch.empty_like(t) for t in batch.images_out]
+    sino_out = [torch.empty_like(t) for t in batch.sinos_out]
+    arr = _noalloc_scans(batch, img_out, sino_out)
+    assert len(arr) == 64
+    gen = torch.Generator(device=DEV).manual_seed(7)
+    for t in batch.images_in + batch.sinos_in:
+        t.copy_(torch.rand(t.shape, generator=gen, device=DEV))
+    for t in img_out + sino_out:
+        t.fill_(float("nan"))
+    batch.forward()
+    batch.back()
+    bt, ctas = batch.config["block_threads"], batch.config["n_cta"]
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for adjoint in (0, 1):
+        assert N.lib.ctlab_project_batched_noalloc(arr, 64, adjoint, 0, bt, ctas, stream) == 0, \
+            N.lib.ctlab_last_error()
     torch.cuda.synchronize()
+    for i in range(64):
+        assert not torch.isnan(sino_out[i]).any() and not torch.isnan(img_out[i]).any(), i
+        assert _rel(sino_out[i], batch.sinos_out[i]) <= TOL, i
+        assert _rel(img_out[i], batch.images_out[i]) <= TOL, i
