@@ -11,9 +11,13 @@ GRays/s fwd+adj = rays / (t_fwd + t_adj) / 1e9.
 ours (default): device-resident timing with CUDA events on the launching
 stream, W untimed warm-up steps, then K timed steps; L2 is flushed (a
 512 MiB write) before every timed step and the flush is not timed.  With
-N > 1 (torchrun, one process per GPU) every rank projects its own full scan
-(independent scans, weak scaling, no collective on the data path) and the
-time is the max over ranks.  Rank 0 prints one JSON line that also holds:
+N > 1 (torchrun, one process per GPU) the scan's views are split across the
+ranks (RaySharded3DProjector: each rank projects its whole views, the forward
+all-gathers the sinogram shards and the adjoint all-reduces the partial
+volumes over NCCL; strong scaling, one scan per job; --sharded takes the same
+path on one GPU); --replicas instead gives every rank its own whole scan
+(weak scaling, no collective).  The time is the max over ranks.  Rank 0
+prints one JSON line that also holds:
   roofline      dominant kernel: algorithmic bytes / mean launch time vs the
                 measured HBM copy bandwidth (MEASURED_PEAKS.json)
   cpu_baseline  the CPU port of the reference's torch path (oracle/) on this
@@ -142,12 +146,24 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 or (args.sharded and args.impl == "ours"):
         import datetime
+        import socket
         import torch.distributed as dist
         backend = "nccl" if args.impl == "ours" else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
+            # NCCL's communicator set-up lines (ranks, transports) on stderr
+            os.environ.setdefault("NCCL_DEBUG", "INFO")
+            os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+        if world == 1:  # a one-rank group for the sharded path on one GPU
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            if "MASTER_PORT" not in os.environ:
+                with socket.socket() as sk:
+                    sk.bind(("127.0.0.1", 0))
+                    os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     elif args.impl == "ours":
         torch.cuda.set_device(local)
@@ -316,6 +332,15 @@ def run_ours(args, world, rank, local):
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
                                   pixel_size=w.pixel, device=dev)
     n_ray = proj.src.shape[0]
+    shard = (0, n_ray)
+    base = proj  # the whole scan's projector (the CPU and MAP legs use it)
+    if args.sharded:
+        # one scan, its views split across the ranks: all-gather of the
+        # sinogram shards (forward), all-reduce of the partial volumes (adjoint)
+        from ct_laboratory_b200.sharded import RaySharded3DProjector
+        proj = RaySharded3DProjector(proj)
+        shard = (proj.lo, proj.hi)
+    rays_per_step = n_ray if args.sharded else world * n_ray  # the whole job's rays
     x = w.phantom(device=dev)
     y = torch.rand(n_ray, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -350,10 +375,14 @@ def run_ours(args, world, rank, local):
     t_adj = np.array([e[1].elapsed_time(e[2]) for e in ev])
     total_ms = float((t_fwd + t_adj).sum())
     total_ms = max_over_ranks(total_ms, world)
-    value = world * n_ray * args.steps / (total_ms / 1e3) / 1e9
+    value = rays_per_step * args.steps / (total_ms / 1e3) / 1e9
 
     peak, peak_src = peaks()
     bytes_per_launch, seg = algorithmic_bytes(w.name, n_ray)
+    if args.sharded and bytes_per_launch:
+        # this rank's share of the scan's bytes (views carry nearly equal
+        # segment counts); its launch times include the collectives
+        bytes_per_launch = bytes_per_launch * (shard[1] - shard[0]) / n_ray
     kern = {}
     for name, t in (("forward", t_fwd), ("adjoint", t_adj)):
         ms = float(t.mean())
@@ -366,10 +395,10 @@ def run_ours(args, world, rank, local):
                 "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "segments": seg, "kernels": kern}
 
-    e2e = run_e2e(proj, x, y, args, dev, w, world) if args.e2e_steps > 0 else None
+    e2e = run_e2e(proj, x, y, args, dev, w, world, rays_per_step) if args.e2e_steps > 0 else None
     batched = run_batched(args, dev, flush) if (world == 1 and args.batched_steps > 0) else None
     serving = run_serving(args, dev) if (world == 1 and args.serve_jobs > 0) else None
-    map_leg = run_map(args, dev, proj, x, y) if (world == 1 and args.map_iters > 0 and w.name.startswith("cone")) \
+    map_leg = run_map(args, dev, base, x, y) if (world == 1 and args.map_iters > 0 and w.name.startswith("cone")) \
         else None
     cpu = None
     if world == 1 and rank == 0 and args.cpu_baseline_s > 0:
@@ -379,20 +408,24 @@ def run_ours(args, world, rank, local):
             with torch.no_grad():
                 y0 = torch.zeros_like(y)
                 y0[:pv] = y[:pv]
-                view0 = (proj.forward_project(x)[:pv].cpu().numpy(), proj.back_project(y0).cpu().numpy(),
+                view0 = (base.forward_project(x)[:pv].cpu().numpy(), base.back_project(y0).cpu().numpy(),
                          y[:pv].cpu().numpy())
-        cpu = cpu_baseline(CpuCase(w, proj.src, proj.dst, proj.M, proj.b, x), args.cpu_baseline_s, view0)
+        cpu = cpu_baseline(CpuCase(w, base.src, base.dst, base.M, base.b, x), args.cpu_baseline_s, view0)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "GRays/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "scaling": "strong" if args.sharded else "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic",
                "config": {"workload": w.name, "n_ray": n_ray, "volume": list(w.n),
-                          "views": w.n_view, "rays_per_rank": n_ray, "l2": "flushed (512 MiB write) before each step",
+                          "views": w.n_view, "rays_per_rank": shard[1] - shard[0],
+                          "l2": "flushed (512 MiB write) before each step",
                           "tile_rows": args.tile_rows, "block_threads": args.block_threads,
                           "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
                           "walk": ["auto", "lane", "column"][args.walk],
                           "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
-                          "parallelism": f"independent scans x{world}"},
+                          "parallelism": (f"ray-sharded x{world}: one scan, whole views per rank, NCCL "
+                                          "all-gather (forward) and all-reduce (adjoint)") if args.sharded
+                          else f"independent scans x{world}"},
                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "batched": batched,
                "serving": serving, "map": map_leg,
                "gpu_launches": launches_per_step * args.steps}
@@ -408,7 +441,7 @@ def _fwd3(proj, x):
     return proj.forward_project(x)
 
 
-def run_e2e(proj, x, y, args, dev, w, world=1):
+def run_e2e(proj, x, y, args, dev, w, world=1, rays_per_step=None):
     """Public API, host buffers: H2D of the volume and of the adjoint input,
     D2H of the sinogram and of the back-projection, every step.  The device
     inputs are double-buffered and each copy direction has its own stream
@@ -465,10 +498,11 @@ def run_e2e(proj, x, y, args, dev, w, world=1):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         barrier(world)
-    # every rank runs its own scan: the job's time is the slowest rank's
+    # the job's time is the slowest rank's
     ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
     n_ray = y.numel()
-    return {"value": world * n_ray / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
+    rays = world * n_ray if rays_per_step is None else rays_per_step
+    return {"value": rays / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
             "h2d_bytes_per_step": int(world * (x_h.numel() * 4 + y_h.numel() * 4)),
             "d2h_bytes_per_step": int(world * (sino_h.numel() * 4 + vol_h.numel() * 4)),
             "api": f"{type(proj).__name__}.__call__ + .back_project" +
@@ -685,6 +719,10 @@ def main():
     ap.add_argument("--voxel-rule", type=int, default=0, help="0 = reference midpoint rule, 1 = crossing rule")
     ap.add_argument("--walk", type=int, default=0, help="0 = auto, 1 = per-lane walk, 2 = column walk")
     ap.add_argument("--deterministic", action="store_true", help="adjoint by the voxel-driven gather")
+    ap.add_argument("--sharded", action="store_true",
+                    help="split one scan's views across the ranks (the default when N > 1; with N = 1 the "
+                         "same path over a one-rank group)")
+    ap.add_argument("--replicas", action="store_true", help="N > 1: every rank projects its own whole scan")
     ap.add_argument("--views", type=int, default=0,
                     help="override the workload's view count (smaller cases for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=10)
@@ -700,6 +738,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not args.replicas and not args.workload.startswith("fan"):
+        args.sharded = True
+    if args.workload.startswith("fan"):
+        args.sharded = False  # the ray-sharded projector is 3-D
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
@@ -707,7 +749,7 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 or (args.sharded and args.impl == "ours"):
             import torch.distributed as dist
             dist.destroy_process_group()
 
