@@ -30,7 +30,7 @@ prints one JSON line that also holds:
 and, at N = 1, three legs of the other workloads (each can be switched off):
   batched       64 uneven 2-D scans: one persistent launch per direction from
                 a CUDA graph against the per-scan loop (--batched-steps 0)
-  serving       16 MAP jobs arriving at 20/s: the continuous-batching server
+  serving       100 MAP jobs arriving at 20/s: the continuous-batching server
                 against the plain per-job estimator loop (--serve-jobs 0)
   map           MAP on the cone scan: Lanczos k=64 preconditioner, 50
                 iterations, finite-difference gradient check, adjoint
@@ -589,11 +589,19 @@ def run_serving(args, dev):
     jobs = make_jobs(w, dev)
     make_s = time.perf_counter() - t0
     plain = sequential_baseline(jobs, dev)
-    server_all = ReconServer(dev, policy="all")
-    sa = latency_summary(server_all.run(jobs))
+    sa = None
+    if args.serve_policy_all:
+        server_all = ReconServer(dev, policy="all")
+        sa = latency_summary(server_all.run(jobs))
     server = ReconServer(dev, policy="srpt")
     served = server.run(jobs)
     ps, ss = latency_summary(plain), latency_summary(served)
+    # the projector work every schedule on this GPU must do: each job's
+    # iterations x its measured forward + adjoint pair
+    work_s = sum(j.iters * j.pair_ms for j in jobs) / 1e3
+    geo = {}
+    for j in jobs:
+        geo[(j.n, j.views)] = geo.get((j.n, j.views), 0) + 1
     xs = {r["job_id"]: r["x"] for r in served}
     rel = []
     for r in plain:
@@ -607,6 +615,13 @@ def run_serving(args, dev):
             "rays_x_iters": sum(j.n_ray * j.iters for j in jobs),
             "plain_loop": ps, "served": ss, "served_all_every_tick": sa,
             "throughput_ratio": ss["jobs_per_s"] / ps["jobs_per_s"],
+            "projector_work_s": work_s,
+            "throughput_ratio_bound": ps["makespan_s"] / work_s,
+            "served_breakdown_s": {"projector_launches": server.log[-1]["projector_s"],
+                                   "per_job_elementwise": server.log[-1]["elementwise_s"],
+                                   "host_and_idle": ss["makespan_s"] - server.log[-1]["projector_s"]
+                                   - server.log[-1]["elementwise_s"]},
+            "jobs_sharing_a_geometry": sum(c for c in geo.values() if c > 1),
             "p50_ratio": ss["p50_s"] / ps["p50_s"], "p99_ratio": ss["p99_s"] / ps["p99_s"],
             "max_rel_rmse_served_vs_plain": max(rel),
             "served_max_active": server.log[-1]["max_active"], "served_ticks": server.log[-1]["ticks"],
@@ -614,7 +629,11 @@ def run_serving(args, dev):
             "note": "plain loop = ConeBeam3DProjector + MaximumAPosterioriEstimator per job in arrival order; "
                     "served = ReconServer, policy srpt (admission by HBM budget; each tick one batched forward and "
                     "adjoint launch over the active jobs with the least remaining work, >= 64M rays); "
-                    "served_all_every_tick = the same server advancing every active job each tick"}
+                    "served_all_every_tick = the same server advancing every active job each tick "
+                    "(--serve-policy-all); projector_work_s = sum over jobs of iterations x one measured forward + "
+                    "adjoint pair of the job's scan, so throughput_ratio_bound = plain makespan / that work bounds "
+                    "any schedule of these projector calls on this GPU; jobs_sharing_a_geometry = jobs whose "
+                    "(volume, views) another job also has (only those could share one multi-volume walk)"}
 
 
 def run_map(args, dev, proj, x_true, y_rand):
@@ -729,8 +748,10 @@ def main():
     ap.add_argument("--map-iters", type=int, default=50, help="MAP iterations on the cone scan (0 = skip the leg)")
     ap.add_argument("--map-k", type=int, default=64, help="eigenpairs of the Lanczos preconditioner")
     ap.add_argument("--lanczos-restarts", type=int, default=8)
-    ap.add_argument("--serve-jobs", type=int, default=16,
+    ap.add_argument("--serve-jobs", type=int, default=100,
                     help="jobs of the MAP serving workload (0 = skip that leg)")
+    ap.add_argument("--serve-policy-all", action="store_true",
+                    help="also serve with every active job advancing each tick")
     ap.add_argument("--batched-steps", type=int, default=10,
                     help="timed passes of the 64-scan batched workload (0 = skip that leg)")
     ap.add_argument("--cpu-baseline-s", type=float, default=15.0)

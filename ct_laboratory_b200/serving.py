@@ -72,6 +72,7 @@ class JobSpec:
     sdd: float = 1500.0
     prior_w: float = 1e-2
     y: torch.Tensor = field(default=None, repr=False)
+    pair_ms: float = 0.0  # one forward + adjoint of this job's scan on the device (make_jobs measures it)
 
     @property
     def n_ray(self):
@@ -111,6 +112,12 @@ def make_jobs(workload, device, lr_scale=1.0):
             y = torch.poisson(spec.I0 * torch.exp(-line), generator=g)
             row = float(p.forward_project(torch.ones_like(x)).max())
             col = float(p.back_project(torch.ones_like(line)).max())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            p.back_project(p.forward_project(x))
+            e1.record()
+            e1.synchronize()
+            spec.pair_ms = e0.elapsed_time(e1)
         spec.lr = lr_scale / (spec.I0 * row * col)
         spec.y = y.cpu().pin_memory()
         jobs.append(spec)
@@ -195,6 +202,7 @@ class ReconServer:
         batch, dirty, batch_key = None, True, None
         ticks = deque()
         n_ticks = peak = 0
+        marks = []  # per tick: events before / after the projector and elementwise phases
         t0 = time.perf_counter() if t0 is None else t0
         with torch.no_grad(), torch.cuda.device(dev):
             while queue or active or finishing:
@@ -233,13 +241,20 @@ class ReconServer:
                     batch_key, dirty = key, False
                 if len(ticks) >= self.run_ahead:  # bound how far the host runs ahead of the GPU
                     ticks.popleft().synchronize()
+                m = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+                m[0].record()
                 batch.forward()
+                m[1].record()
                 for a in sel:
                     _residual_(a)
+                m[2].record()
                 batch.back()
+                m[3].record()
                 for a in sel:
                     _prior_and_step_(a)
                     a.it += 1
+                m[4].record()
+                marks.append(m)
                 ev = torch.cuda.Event()
                 ev.record()
                 ticks.append(ev)
@@ -260,7 +275,11 @@ class ReconServer:
                         used -= a.nbytes
                     del a
                     dirty = True
-        self.log.append({"ticks": n_ticks, "max_active": peak})
+        torch.cuda.synchronize(dev)
+        proj_ms = sum(m[0].elapsed_time(m[1]) + m[2].elapsed_time(m[3]) for m in marks)
+        elem_ms = sum(m[1].elapsed_time(m[2]) + m[3].elapsed_time(m[4]) for m in marks)
+        self.log.append({"ticks": n_ticks, "max_active": peak, "projector_s": proj_ms / 1e3,
+                         "elementwise_s": elem_ms / 1e3})
         out = []
         for jid in sorted(results):
             r = results[jid]

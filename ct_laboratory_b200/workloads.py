@@ -174,7 +174,7 @@ class ScanBatchWorkload:
 class ServingWorkload:
     """MAP reconstruction requests arriving as a seeded Poisson process."""
     name: str = "serve"
-    n_jobs: int = 16
+    n_jobs: int = 100
     rate: float = 20.0
     sizes: tuple = (128, 256, 384)
     probs: tuple = (0.5, 0.35, 0.15)
