@@ -70,6 +70,7 @@ def rnd(shape, seed):
 def run_reference_layers(tomo, workdir):
     """Seeded calls through the reference's classes and functions; returns
     numpy results keyed by name (and leaves its table files in workdir)."""
+    os.makedirs(workdir, exist_ok=True)  # (the reference's save_tvals expects the directory)
     out = {}
     cone = tomo.ConeBeam3DProjector(**CONE, backend="cuda", device=DEV)
     n = (CONE["n_x"], CONE["n_y"], CONE["n_z"])
