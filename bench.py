@@ -327,7 +327,7 @@ def run_ours(args, world, rank, local):
                                    deterministic_adjoint=args.deterministic, block_threads=args.block_threads)
     elif w.name.startswith("static"):
         # StaticCT ring: the modules' 16-row columns take the column walk
-        proj = w.projector(dev, voxel_rule=args.voxel_rule)
+        proj = w.projector(dev, voxel_rule=args.voxel_rule, deterministic_adjoint=args.deterministic or False)
     else:
         proj = FanBeam2DProjector(*w.n, n_view=w.n_view, n_det=w.n_det, sid=w.sid, sdd=w.sdd, det_spacing=w.pitch,
                                   pixel_size=w.pixel, device=dev)
@@ -345,7 +345,9 @@ def run_ours(args, world, rank, local):
     y = torch.rand(n_ray, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
-    launches_per_step = 2
+    # our kernels per step: the forward walk, then the adjoint's -- one walk
+    # (atomic scatter); ray table + gather; or max|y|, scale, walk, convert
+    launches_per_step = 1 + {None: 1, "gather": 2, "fixed": 4}[args.deterministic]
 
     def fwd():
         return _fwd3(proj, x) if w.name.startswith(("cone", "static")) else proj.forward_project(x)
@@ -422,7 +424,8 @@ def run_ours(args, world, rank, local):
                           "tile_rows": args.tile_rows, "block_threads": args.block_threads,
                           "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
                           "walk": ["auto", "lane", "column"][args.walk],
-                          "adjoint": "gather (deterministic)" if args.deterministic else "atomic scatter",
+                          "adjoint": {None: "float atomic scatter", "gather": "voxel gather (reproducible)",
+                                      "fixed": "64-bit fixed-point scatter (reproducible)"}[args.deterministic],
                           "parallelism": (f"ray-sharded x{world}: one scan, whole views per rank, NCCL "
                                           "all-gather (forward) and all-reduce (adjoint)") if args.sharded
                           else f"independent scans x{world}"},
@@ -737,7 +740,9 @@ def main():
     ap.add_argument("--block-threads", type=int, default=128, help="threads per CTA of the cone-beam launches")
     ap.add_argument("--voxel-rule", type=int, default=0, help="0 = reference midpoint rule, 1 = crossing rule")
     ap.add_argument("--walk", type=int, default=0, help="0 = auto, 1 = per-lane walk, 2 = column walk")
-    ap.add_argument("--deterministic", action="store_true", help="adjoint by the voxel-driven gather")
+    ap.add_argument("--deterministic", nargs="?", const="fixed", default=None, choices=["fixed", "gather"],
+                    help="reproducible adjoint: 'fixed' (default; the forward's walk scattering in 64-bit fixed "
+                         "point) or 'gather' (voxel-driven, crossing rule)")
     ap.add_argument("--sharded", action="store_true",
                     help="split one scan's views across the ranks (the default when N > 1; with N = 1 the "
                          "same path over a one-rank group)")

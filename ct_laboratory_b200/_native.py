@@ -93,6 +93,7 @@ _SIGS = {
     "ctlab_back_project_batched": [_BP, _I, _I32, _P],
     "ctlab_batch_default_ctas": [_I32, _I, _I, _I32, ctypes.POINTER(_I32)],
     "ctlab_project_batched_noalloc": [_SP, _I32, _I, _I, _I32, _I32, _P],
+    "ctlab_back_project_3d_fixed": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P, _I64, _P],
 }
 
 for _name, _args in _SIGS.items():
@@ -106,13 +107,16 @@ lib.ctlab_abi_version.restype = ctypes.c_int
 lib.ctlab_abi_version.argtypes = []
 lib.ctlab_batch_workspace_bytes.restype = ctypes.c_int64
 lib.ctlab_batch_workspace_bytes.argtypes = [_I32]
+lib.ctlab_back_project_3d_fixed_workspace_bytes.restype = ctypes.c_int64
+lib.ctlab_back_project_3d_fixed_workspace_bytes.argtypes = [_I64, _I64, _I64, _I64]
 
 ABI_VERSION = lib.ctlab_abi_version()
 
 
 def exported_symbols():
     """Names of the C entry points this binding declares."""
-    return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version", "ctlab_batch_workspace_bytes"]
+    return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version", "ctlab_batch_workspace_bytes",
+                            "ctlab_back_project_3d_fixed_workspace_bytes"]
 
 
 def call(name: str, *args) -> None:

@@ -20,7 +20,9 @@ from a device work counter (libctlab_b200.so
 direction with its own plan and tile layout.  ``forward_loop()`` / ``back_loop()`` run the very same
 walks one scan at a time through the single-scan entry points, into the
 same buffers: the per-instance loop the batch replaces.  Forward results are
-bitwise equal between the two; adjoints up to the order of float atomics.
+bitwise equal between the two; adjoints up to the order of float atomics,
+or bitwise with ``deterministic_adjoint=True`` (3-D: each scan's adjoint
+scatters in 64-bit fixed point, scan by scan).
 
 Each direction has a mode: the persistent launch, or the loop of
 single-scan launches (the default for the 3-D forward, where the
@@ -127,7 +129,7 @@ def _cost(p):
 
 class ScanBatch:
     def __init__(self, projectors, voxel_rule=N.VOXEL_CROSSING, forward=True, adjoint=True, block_threads=256,
-                 kind="auto", buffers=None):
+                 kind="auto", buffers=None, deterministic_adjoint=False):
         self.projectors = list(projectors)
         if not self.projectors:
             raise ValueError("ScanBatch needs at least one projector")
@@ -140,6 +142,17 @@ class ScanBatch:
             raise RuntimeError("ScanBatch: projectors must live on a CUDA device (there is no CPU implementation)")
         self.voxel_rule = int(voxel_rule)
         self.has_forward, self.has_adjoint = bool(forward), bool(adjoint)
+        # reproducible adjoint (3-D): every scan's walk scatters in 64-bit fixed
+        # point (ctlab_back_project_3d_fixed) into one int64 workspace reused
+        # scan after scan, so a scan's volume is the same bits whichever other
+        # scans share the batch
+        self.deterministic_adjoint = bool(deterministic_adjoint)
+        self._fixed_ws = None
+        if self.deterministic_adjoint and adjoint:
+            if self.ndim != 3:
+                raise ValueError("ScanBatch: deterministic_adjoint is implemented for 3-D scans")
+            need = max(int(N.lib.ctlab_back_project_3d_fixed_workspace_bytes(1, *_dims(p))) for p in self.projectors)
+            self._fixed_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
         shapes = [_dims(p) for p in self.projectors]
         n_rays = [int(p.src.shape[0]) for p in self.projectors]
         if buffers is None:
@@ -260,6 +273,8 @@ class ScanBatch:
                            int(block_threads), ctypes.byref(v))
                     ctas = v.value
             m = mode if mode != "auto" else ("loop" if d == "fwd" and self.ndim == 3 else "persistent")
+            if d == "adj" and self._fixed_ws is not None:
+                m = "loop"  # the fixed-point adjoint runs scan by scan
             cfg = {"block_threads": int(block_threads), "kind": k, "n_cta": int(ctas), "mode": m}
             opts = [_opts(self.projectors[i], k if isinstance(k, str) else k[i], self.voxel_rule, block_threads)
                     for i in range(len(self.projectors))]
@@ -316,7 +331,12 @@ class ScanBatch:
         with torch.cuda.device(self.device):
             for i, p in enumerate(self.projectors):
                 o = self._loop_opts_a[i]
-                if self.ndim == 3:
+                if self._fixed_ws is not None:
+                    N.call("ctlab_back_project_3d_fixed", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
+                           N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), N.ptr(self._fixed_ws),
+                           self._fixed_ws.numel(), st)
+                elif self.ndim == 3:
                     N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
                            N.ptr(self.images_out[i]), acc, ctypes.byref(o), st)

@@ -154,6 +154,40 @@ __device__ __forceinline__ void red_add_if(float* addr, float v, bool pred) {
         : "memory");
 }
 
+// red.global.add.u64 under a predicate (two's-complement: signed sums too).
+__device__ __forceinline__ void red_add_u64_if(unsigned long long* addr, long long v, bool pred) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t@p red.global.add.u64 [%0], %1;\n\t}" ::"l"(addr),
+        "l"(v), "r"((int)pred)
+        : "memory");
+}
+
+// How the 3-D adjoint walks accumulate a contribution v into voxel i of a
+// volume: `at` offsets a volume base by `off` voxels, `add` adds.
+//
+// RedF32: float atomics into the float volume (the order of the additions,
+// and so the last bits of a sum, depend on scheduling).
+struct RedF32 {
+    __device__ __forceinline__ float* at(float* base, int64_t off) const { return base + off; }
+    __device__ __forceinline__ void add(float* p, unsigned i, float v, bool pred) const { red_add_if(p + i, v, pred); }
+};
+
+// RedFixed: every contribution rounded once to a multiple of 2^-e
+// (v * scale, scale = 2^e, to the nearest integer) and added as a 64-bit
+// integer.  Integer addition is associative, so a voxel's sum is the same
+// bits in any order: the adjoint is reproducible run to run and whatever
+// else shares the launch.  The volume base holds int64 sums (`p` is its
+// address, typed as float* only to share the walks' signatures).
+struct RedFixed {
+    float scale;
+    __device__ __forceinline__ float* at(float* base, int64_t off) const {
+        return reinterpret_cast<float*>(reinterpret_cast<unsigned long long*>(base) + off);
+    }
+    __device__ __forceinline__ void add(float* p, unsigned i, float v, bool pred) const {
+        red_add_u64_if(reinterpret_cast<unsigned long long*>(p) + i, __float2ll_rn(__fmul_rn(v, scale)), pred);
+    }
+};
+
 // Ray tiling resolved on the host into plain integers for the kernels.
 struct Tiling {
     int64_t n_view, n_row, n_col;

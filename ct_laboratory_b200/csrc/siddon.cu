@@ -206,9 +206,209 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     return launch_status(what);
 }
 
+// ----------------------------------------------------------------------------
+// Reproducible 3-D adjoint: the walks' contributions added as 64-bit
+// integers (RedFixed), then converted to float once per voxel.
+// ----------------------------------------------------------------------------
+
+// The column walks (either voxel rule) over one sinogram per blockIdx.y,
+// into its int64 volume.
+template <bool MID, int W>
+__global__ void __launch_bounds__(256, CTLAB_XY_MIN_BLOCKS)
+    siddon3d_fixed_column_kernel(const float* __restrict__ in, float* __restrict__ sums,
+                                 const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
+                                 const float* __restrict__ M_inv, const float* __restrict__ bvec, GridDims<3> G,
+                                 int64_t nvox, Tiling T, const float* __restrict__ scale) {
+    const Affine3 A = load_affine3(M_inv, bvec);
+    const RedFixed acc{scale[blockIdx.y]};
+    if constexpr (MID) {
+        __shared__ float raw[256 / 32][kChunk];
+        __shared__ MidCell rec[256 / 32][kChunk];
+        shared_xy_ray_mid<true, 1, W, RedFixed>(in, sums, src, dst, n_ray, A, G, nvox, tile_ray(T), blockIdx.y, 1,
+                                                raw[threadIdx.x >> 5], rec[threadIdx.x >> 5], acc);
+    } else {
+        __shared__ XYCell cells[256 / 32][kChunk];
+        shared_xy_ray<true, 1, W, RedFixed>(in, sums, src, dst, n_ray, A, G, nvox, tile_ray(T), blockIdx.y, 1,
+                                            cells[threadIdx.x >> 5], acc);
+    }
+}
+
+// The per-lane walk (flat or irregular ray lists).
+template <bool MID>
+__global__ void __launch_bounds__(256) siddon3d_fixed_lane_kernel(
+    const float* __restrict__ in, float* __restrict__ sums, const float* __restrict__ src,
+    const float* __restrict__ dst, int64_t n_ray, const float* __restrict__ M_inv, const float* __restrict__ bvec,
+    GridDims<3> G, int64_t nvox, Tiling T, const float* __restrict__ scale) {
+    const int64_t r = tile_ray(T);
+    if (r < 0) return;
+    lane_ray<3, true, MID, RedFixed>(in, sums, src, dst, n_ray, load_affine3(M_inv, bvec), G, nvox, r, blockIdx.y,
+                                     RedFixed{scale[blockIdx.y]});
+}
+
+// max |y| of each sinogram (blockIdx.y) as float bits: for non-negative
+// floats the bit patterns order as the values do, so an unsigned atomicMax
+// gives the same result in any order.
+__global__ void __launch_bounds__(256) abs_max_kernel(const float* __restrict__ y, int64_t n_ray,
+                                                      unsigned* __restrict__ out) {
+    const int64_t b = blockIdx.y;
+    unsigned m = 0u;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_ray; i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, __float_as_uint(fabsf(y[b * n_ray + i])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m != 0u) atomicMax(out + b, m);
+}
+
+// scale = 2^e per sinogram, e the largest integer with B * 2^e <= 2^61 for
+// B = max|y| * L * n_ray, L the longest chord through the grid (the longest
+// of the four world-space body diagonals of the box, M (+-n_x, +-n_y, n_z),
+// with M the inverse of M^-1).  Every contribution |y| * (segment length) is
+// at most max|y| * L and every voxel's sum at most B, so each contribution
+// converts to an int64 below 2^61 and every sum stays below 2^61.  A
+// sinogram holding NaN or inf gets a NaN scale (its volume comes out NaN).
+// The sums are exact modulo 2^64: a partial sum that wraps past 2^63 on the
+// way (pass 1's whole-cell terms before pass 2 takes them back) still ends
+// at the exact final sum.
+__global__ void fixed_scale_kernel(const unsigned* __restrict__ maxbits, int batch, const float* __restrict__ M_inv,
+                                   GridDims<3> G, int64_t n_ray, float* __restrict__ scale) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    double a[9];
+    for (int i = 0; i < 9; ++i) a[i] = M_inv[i];
+    const double c0 = a[4] * a[8] - a[5] * a[7], c1 = a[5] * a[6] - a[3] * a[8], c2 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+    // M = adj(M^-1) / det (columns of the adjugate as rows: M[r][c] = cof[c][r] / det)
+    const double m[9] = {c0 / det, (a[2] * a[7] - a[1] * a[8]) / det, (a[1] * a[5] - a[2] * a[4]) / det,
+                         c1 / det, (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
+                         c2 / det, (a[1] * a[6] - a[0] * a[7]) / det, (a[0] * a[4] - a[1] * a[3]) / det};
+    double L = 0.0;
+    for (int sx = -1; sx <= 1; sx += 2)
+        for (int sy = -1; sy <= 1; sy += 2) {
+            const double v[3] = {sx * (double)G.n[0], sy * (double)G.n[1], (double)G.n[2]};
+            double q = 0.0;
+            for (int r = 0; r < 3; ++r) {
+                const double w = m[3 * r] * v[0] + m[3 * r + 1] * v[1] + m[3 * r + 2] * v[2];
+                q += w * w;
+            }
+            L = fmax(L, sqrt(q));
+        }
+    const float ymax = __uint_as_float(maxbits[b]);
+    const double bound = (double)ymax * L * (double)(n_ray > 0 ? n_ray : 1) * (1.0 + 1e-6);
+    float out = 1.f;
+    if (!isfinite(ymax) || !isfinite(bound)) {
+        out = __int_as_float(0x7fc00000);
+    } else if (bound > 0.0) {
+        const int e = 61 - (int)ceil(log2(bound));
+        // a bound beyond 2^181 has no float scale: the volume comes out NaN
+        out = e < -120 ? __int_as_float(0x7fc00000) : ldexpf(1.f, min(e, 120));
+    }
+    scale[b] = out;
+}
+
+// out = sums / scale (exact in double: scale is a power of 2), rounded to
+// float once; accumulate adds it to out.
+__global__ void __launch_bounds__(256) fixed_to_float_kernel(const long long* __restrict__ sums,
+                                                             const float* __restrict__ scale, int64_t nvox,
+                                                             int64_t total, float* __restrict__ out, int accumulate) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = (float)((double)sums[i] / (double)scale[i / nvox]);
+        out[i] = accumulate ? out[i] + v : v;
+    }
+}
+
+// Bytes of the reproducible adjoint's workspace: a 256-byte-aligned header
+// (per sinogram its max |y| bits and its scale) and an int64 volume per
+// sinogram.
+static int64_t fixed_header_bytes(int64_t batch) { return ((batch * 8 + 255) / 256) * 256; }
+
 }  // namespace ctlab
 
 using namespace ctlab;
+
+extern "C" int64_t ctlab_back_project_3d_fixed_workspace_bytes(int64_t batch, int64_t n_x, int64_t n_y,
+                                                               int64_t n_z) {
+    if (batch < 1 || n_x < 1 || n_y < 1 || n_z < 1) return -1;
+    return fixed_header_bytes(batch) + batch * n_x * n_y * n_z * 8;
+}
+
+extern "C" int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                           const float* dst, const float* M_inv, const float* b, int64_t n_x,
+                                           int64_t n_y, int64_t n_z, float* out, int accumulate,
+                                           const ctlab_ray_opts* tiling, void* workspace, int64_t workspace_bytes,
+                                           void* stream) {
+    clear_error();
+    const char* what = "back_project_3d_fixed";
+    CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535], got %lld", what, (long long)batch);
+    CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
+    const int64_t dims[3] = {n_x, n_y, n_z};
+    GridDims<3> G;
+    int64_t nvox = 1, st = 1;
+    for (int a = 0; a < 3; ++a) {
+        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] <= (1 << 22), "%s: grid dimension %d out of range (%lld)", what, a,
+                      (long long)dims[a]);
+        nvox *= dims[a];
+    }
+    CTLAB_REQUIRE(nvox < (1LL << 31), "%s: a volume of %lld voxels exceeds 2^31", what, (long long)nvox);
+    for (int a = 2; a >= 0; --a) {
+        G.n[a] = (int)dims[a];
+        G.stride[a] = (int)st;
+        st *= dims[a];
+    }
+    CTLAB_REQUIRE(out && M_inv && b, "%s: null data pointer", what);
+    CTLAB_REQUIRE(n_ray == 0 || (src && dst && sino), "%s: null src/dst/sinogram", what);
+    const int64_t need = ctlab_back_project_3d_fixed_workspace_bytes(batch, n_x, n_y, n_z);
+    CTLAB_REQUIRE(workspace != nullptr && workspace_bytes >= need && ((uintptr_t)workspace & 255) == 0,
+                  "%s: workspace must be 256-byte aligned and hold %lld bytes (got %lld)", what, (long long)need,
+                  (long long)workspace_bytes);
+    cudaStream_t s = as_stream(stream);
+    unsigned* maxbits = reinterpret_cast<unsigned*>(workspace);
+    float* scale = reinterpret_cast<float*>(maxbits + batch);
+    long long* sums = reinterpret_cast<long long*>(reinterpret_cast<char*>(workspace) + fixed_header_bytes(batch));
+    CTLAB_CUDA_TRY(cudaMemsetAsync(workspace, 0, (size_t)need, s));
+    if (n_ray > 0) {
+        const int64_t per = (n_ray + 255) / 256;
+        abs_max_kernel<<<dim3((unsigned)(per < 4096 ? per : 4096), (unsigned)batch), 256, 0, s>>>(sino, n_ray, maxbits);
+        int rc = launch_status(what);
+        if (rc) return rc;
+    }
+    fixed_scale_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, s>>>(maxbits, (int)batch, M_inv, G, n_ray, scale);
+    int rc = launch_status(what);
+    if (rc) return rc;
+    if (n_ray > 0) {
+        Tiling T;
+        rc = resolve_tiling(tiling, n_ray, T);
+        if (rc) return rc;
+        CTLAB_REQUIRE(T.n_blocks <= kMaxGrid, "%s: too many rays for one launch", what);
+        const int threads = T.tile_rows * T.tile_cols;
+        const bool mid = tiling == nullptr || tiling->voxel_rule == CTLAB_VOXEL_MIDPOINT;
+        const bool flat = tiling == nullptr || tiling->n_view == 0;
+        const int walk = tiling == nullptr ? CTLAB_WALK_AUTO : tiling->walk;
+        const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
+        const dim3 g((unsigned)T.n_blocks, (unsigned)batch);
+        float* o = reinterpret_cast<float*>(sums);
+        if (!flat && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
+            (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
+            if (T.tile_rows == 16) {
+                if (mid) siddon3d_fixed_column_kernel<true, 16><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+                else siddon3d_fixed_column_kernel<false, 16><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+            } else {
+                if (mid) siddon3d_fixed_column_kernel<true, 32><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+                else siddon3d_fixed_column_kernel<false, 32><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+            }
+        } else if (mid) {
+            siddon3d_fixed_lane_kernel<true><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+        } else {
+            siddon3d_fixed_lane_kernel<false><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
+        }
+        rc = launch_status(what);
+        if (rc) return rc;
+    }
+    const int64_t total = batch * nvox;
+    const int64_t blocks = (total + 255) / 256;
+    fixed_to_float_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, s>>>(sums, scale, nvox, total,
+                                                                                            out, accumulate);
+    return launch_status(what);
+}
 
 extern "C" int ctlab_forward_project_3d_on_the_fly_ex(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
                                                       int64_t n_z, const float* src, const float* dst,

@@ -165,10 +165,12 @@ constexpr int kLaneSteps = CTLAB_LANE_STEPS;
 // ADJ=true: scatters y*len into out[voxel].  MID selects the voxel of each
 // segment: true = the reference's rounded world midpoint, false = the voxel
 // between the two crossings that bound the segment (exact topology).
-template <int NDIM, bool ADJ, bool MID>
+// `acc` accumulates the adjoint's contributions (RedF32 float atomics, or
+// RedFixed integer sums; `out` is then the int64 volume).
+template <int NDIM, bool ADJ, bool MID, class Acc = RedF32>
 __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* __restrict__ out, float y,
                                           const float* sw, const float* dw, const GridDims<NDIM>& G,
-                                          const AffineT<NDIM>& A, unsigned nvox) {
+                                          const AffineT<NDIM>& A, unsigned nvox, const Acc& acc = Acc()) {
     // World direction and length: ct_projector_3d.cu:941-942 (fused as nvcc
     // contracts vx*vx + vy*vy + vz*vz).
     float vw[NDIM];
@@ -342,8 +344,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             for (int a = 0; a < NDIM; ++a) pb[a] = pn[a] - ps[a];
             const int ne = edge_segments<NDIM, -1>(A, sw, vw, s, inv, ps, pb, t_enter, ray_len, G, ev, el);
 #pragma unroll
-            for (int k = 0; k < kEdge; ++k)
-                red_add_if(out + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
+            for (int k = 0; k < kEdge; ++k) acc.add(out, (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
         }
         // Segment length (t1 - t0) * |v| (ct_projector_3d.cu:998) times y;
         // the crossing rule multiplies y * |v| once by each span t1 - t0.
@@ -357,7 +358,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             const float span = __fsub_rn(t1, t_cur);
             const float seg = MID ? __fmul_rn(span, ray_len) : span;
             const int v = MID ? midpoint_voxel<NDIM>(A, sw, vw, t_cur, t1, G) : idx;
-            red_add_if(out + (unsigned)v, __fmul_rn(yl, seg), seg > 0.f && v >= 0);
+            acc.add(out, (unsigned)v, __fmul_rn(yl, seg), seg > 0.f && v >= 0);
             if (!(tm < t_exit)) break;
             t_cur = t1;
 #pragma unroll
@@ -374,8 +375,7 @@ __device__ __forceinline__ float traverse(const float* __restrict__ vol, float* 
             int ev[kEdge];
             const int ne = edge_segments<NDIM, 1>(A, sw, vw, s, inv, ps, pn, t_exit, ray_len, G, ev, el);
 #pragma unroll
-            for (int k = 0; k < kEdge; ++k)
-                red_add_if(out + (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
+            for (int k = 0; k < kEdge; ++k) acc.add(out, (unsigned)ev[k], __fmul_rn(y, el[k]), k < ne && el[k] > 0.f);
         }
         return 0.f;
     }
@@ -746,11 +746,11 @@ __device__ __forceinline__ void major2_adjoint_warp(const float* __restrict__ in
 #endif
 
 // Per-thread body of the per-lane walk: ray r (>= 0) of batch item bi.
-template <int NDIM, bool ADJ, bool MID>
+template <int NDIM, bool ADJ, bool MID, class Acc = RedF32>
 __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __restrict__ out,
                                          const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
                                          const AffineT<NDIM>& aff, const GridDims<NDIM>& G, int64_t nvox, int64_t r,
-                                         int64_t bi) {
+                                         int64_t bi, const Acc& acc = Acc()) {
     float sw[NDIM], dw[NDIM];
 #pragma unroll
     for (int a = 0; a < NDIM; ++a) {
@@ -763,7 +763,7 @@ __device__ __forceinline__ void lane_ray(const float* __restrict__ in, float* __
         if constexpr (NDIM == 2 && !MID && CTLAB_MAJOR2 >= 1)
             traverse_major2<true>(nullptr, out + bi * nvox, y, sw, dw, G, aff);
         else
-            traverse<NDIM, true, MID>(nullptr, out + bi * nvox, y, sw, dw, G, aff, (unsigned)nvox);
+            traverse<NDIM, true, MID, Acc>(nullptr, acc.at(out, bi * nvox), y, sw, dw, G, aff, (unsigned)nvox, acc);
     } else {
         float v;
         if constexpr (NDIM == 2 && !MID && CTLAB_MAJOR2 >= 2)
@@ -1017,11 +1017,12 @@ __device__ __forceinline__ float accumulate_group(const CellGroup<NG>& g, const 
 // half, with all 32 lanes taking part), a group that has left the volume
 // idling until the other is done; every decision that branches around a
 // collective step is taken for the whole warp.
-template <bool ADJ, int NB, int W = 32>
+template <bool ADJ, int NB, int W = 32, class Acc = RedF32>
 __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, float* __restrict__ out,
                                               const float* __restrict__ src, const float* __restrict__ dst,
                                               int64_t n_ray, const Affine3& A, const GridDims<3>& G,
-                                              int64_t nvox, int64_t r, int64_t b0, int nb, XYCell* buf) {
+                                              int64_t nvox, int64_t r, int64_t b0, int nb, XYCell* buf,
+                                              const Acc& acc = Acc()) {
     static_assert(W == 32 || W == 16, "group width must be 32 or 16");
     const int wlane = threadIdx.x & 31;
     const int lane = wlane & (W - 1);  // lane within the group
@@ -1081,7 +1082,8 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
             if constexpr (ADJ) {
                 const float yj = ld_stream(in + b * n_ray + r);
                 if (R.live && yj != 0.f)
-                    traverse<3, true, false>(nullptr, out + b * nvox, yj, sw, dw, G, A, (unsigned)nvox);
+                    traverse<3, true, false, Acc>(nullptr, acc.at(out, b * nvox), yj, sw, dw, G, A, (unsigned)nvox,
+                                                  acc);
             } else {
                 st_stream(out + b * n_ray + r,
                           R.live ? traverse<3, false, false>(in + b * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
@@ -1158,13 +1160,13 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
     // off), so every address stays inside the batch.
     const float* vol[NB];
     float* vout[NB];
-    float acc[NB], yl[NB];
+    float sum[NB], yl[NB];
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         const int64_t b = b0 + (j < nb ? j : nb - 1);
         vol[j] = ADJ ? nullptr : pin_ptr(in + b * nvox);
-        vout[j] = ADJ ? pin_ptr(out + b * nvox) : nullptr;
-        acc[j] = 0.f;
+        vout[j] = ADJ ? pin_ptr(acc.at(out, b * nvox)) : nullptr;
+        sum[j] = 0.f;
         yl[j] = __fmul_rn(y[j], Z.len);  // adjoint: y * |v| (0 on dead lanes)
     }
     const uint64_t pol = l2_policy_keep();
@@ -1213,8 +1215,8 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
 #pragma unroll
                         for (int u = 0; u < kGroupAdj; ++u) {
                             const bool vj = NB == 1 || j < nb;  // one volume: always valid
-                            red_add_if(vout[j] + g.ia[u], __fmul_rn(yl[j], g.sa[u]), g.sa[u] > 0.f && vj);
-                            red_add_if(vout[j] + g.ib[u], __fmul_rn(yl[j], g.sb[u]), g.sb[u] > 0.f && vj);
+                            acc.add(vout[j], g.ia[u], __fmul_rn(yl[j], g.sa[u]), g.sa[u] > 0.f && vj);
+                            acc.add(vout[j], g.ib[u], __fmul_rn(yl[j], g.sb[u]), g.sb[u] > 0.f && vj);
                         }
                     }
                 }
@@ -1229,7 +1231,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
 #pragma unroll
                     for (int j = 0; j < NB; ++j) gather_group<kGF>(vol[j], g, v[j], pol);
 #pragma unroll
-                    for (int j = 0; j < NB; ++j) acc[j] = accumulate_group<kGF>(g, v[j], acc[j]);
+                    for (int j = 0; j < NB; ++j) sum[j] = accumulate_group<kGF>(g, v[j], sum[j]);
                 }
             }
             if constexpr (W == 32) {
@@ -1257,7 +1259,7 @@ __device__ __forceinline__ void shared_xy_ray(const float* __restrict__ in, floa
         if (r >= 0) {
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(acc[j], Z.len));
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(sum[j], Z.len));
         }
     }
 }
@@ -1347,12 +1349,12 @@ __device__ __forceinline__ int count_le(const float* v, float key) {
 
 // Per-thread body; arguments as shared_xy_ray.  `raw` is the warp's kChunk
 // floats of crossing parameters, `rec` its kChunk cell records.
-template <bool ADJ, int NB, int W = 32>
+template <bool ADJ, int NB, int W = 32, class Acc = RedF32>
 __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, float* __restrict__ out,
                                                   const float* __restrict__ src, const float* __restrict__ dst,
                                                   int64_t n_ray, const Affine3& A, const GridDims<3>& G,
                                                   int64_t nvox, int64_t r, int64_t b0, int nb, float* raw,
-                                                  MidCell* rec) {
+                                                  MidCell* rec, const Acc& acc = Acc()) {
     static_assert(W == 32 || W == 16, "group width must be 32 or 16");
     const int wlane = threadIdx.x & 31;
     const int lane = wlane & (W - 1);
@@ -1412,7 +1414,8 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
             if constexpr (ADJ) {
                 const float yj = ld_stream(in + b * n_ray + r);
                 if (R.live && yj != 0.f)
-                    traverse<3, true, true>(nullptr, out + b * nvox, yj, sw, dw, G, A, (unsigned)nvox);
+                    traverse<3, true, true, Acc>(nullptr, acc.at(out, b * nvox), yj, sw, dw, G, A, (unsigned)nvox,
+                                                 acc);
             } else {
                 st_stream(out + b * n_ray + r,
                           R.live ? traverse<3, false, true>(in + b * nvox, nullptr, 0.f, sw, dw, G, A, (unsigned)nvox)
@@ -1468,13 +1471,13 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
 
     const float* vol[NB];
     float* vout[NB];
-    float acc[NB], yl[NB];
+    float sum[NB], yl[NB];
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
         const int64_t b = b0 + (j < nb ? j : nb - 1);
         vol[j] = ADJ ? nullptr : pin_ptr(in + b * nvox);
-        vout[j] = ADJ ? pin_ptr(out + b * nvox) : nullptr;
-        acc[j] = 0.f;
+        vout[j] = ADJ ? pin_ptr(acc.at(out, b * nvox)) : nullptr;
+        sum[j] = 0.f;
         yl[j] = __fmul_rn(y[j], len);  // adjoint: y * |v|, times each parameter span
     }
     const uint64_t pol = l2_policy_keep();
@@ -1483,9 +1486,9 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
             if constexpr (ADJ) {
-                red_add_if(vout[j] + (unsigned)v, __fmul_rn(yl[j], w), use && (NB == 1 || j < nb));
+                acc.add(vout[j], (unsigned)v, __fmul_rn(yl[j], w), use && (NB == 1 || j < nb));
             } else {
-                if (use) acc[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)v, pol), w, acc[j]);
+                if (use) sum[j] = __fmaf_rn(ld_keep(vol[j] + (unsigned)v, pol), w, sum[j]);
             }
         }
     };
@@ -1573,7 +1576,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
 #pragma unroll
                     for (int j = 0; j < NB; ++j)
 #pragma unroll
-                        for (int u = 0; u < kNG; ++u) acc[j] = uq[u] ? __fmaf_rn(vv[j][u], wq[u], acc[j]) : acc[j];
+                        for (int u = 0; u < kNG; ++u) sum[j] = uq[u] ? __fmaf_rn(vv[j][u], wq[u], sum[j]) : sum[j];
                 }
             }
             // ---- pass 2: this lane's cells with a z plane, entry or exit inside
@@ -1656,7 +1659,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         if (r >= 0) {
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(acc[j], len));
+                if (j < nb) st_stream(out + (b0 + j) * n_ray + r, __fmul_rn(sum[j], len));
         }
     }
 }

@@ -30,7 +30,10 @@ non-periodic quadratic smoothness prior (image_energies.py:18-29):
 
 written out directly instead of through autograd.  A job's result does not
 depend on which other jobs share its launches: the forward is deterministic
-and the adjoint differs only in the order of float atomic additions.
+and the adjoint differs only in the order of float atomic additions -- with
+``deterministic_adjoint=True`` not even that: every job's adjoint scatters
+in 64-bit fixed point (integer sums, associative), so a job served alone and
+the same job served among others give the same bits.
 
 ``sequential_baseline(jobs)`` serves the same jobs one at a time in arrival
 order through the reference-style API (``ConeBeam3DProjector`` +
@@ -160,7 +163,8 @@ def _prior_and_step_(job):
 
 
 class ReconServer:
-    def __init__(self, device, budget_bytes=None, max_active=16, run_ahead=2, policy="srpt", tick_rays=64_000_000):
+    def __init__(self, device, budget_bytes=None, max_active=16, run_ahead=2, policy="srpt", tick_rays=64_000_000,
+                 deterministic_adjoint=False):
         """policy "all": every active job advances one iteration per tick.
         policy "srpt": the active jobs with the least remaining work (rays x
         iterations left) advance, as many as fill `tick_rays` rays per tick
@@ -169,6 +173,7 @@ class ReconServer:
         if policy not in ("all", "srpt"):
             raise ValueError(f"unknown policy {policy!r}")
         self.policy = policy
+        self.deterministic_adjoint = bool(deterministic_adjoint)
         self.tick_rays = int(tick_rays)
         self.device = torch.device(device)
         if budget_bytes is None:
@@ -236,7 +241,7 @@ class ReconServer:
                 key = tuple(id(a) for a in sel)
                 if dirty or key != batch_key:
                     batch = ScanBatch([a.proj for a in sel], voxel_rule=N.VOXEL_CROSSING,
-                                      buffers={"images_in": [a.x for a in sel], "sinos_out": [a.p for a in sel],
+                                      deterministic_adjoint=self.deterministic_adjoint, buffers={"images_in": [a.x for a in sel], "sinos_out": [a.p for a in sel],
                                                "sinos_in": [a.r for a in sel], "images_out": [a.g for a in sel]})
                     batch_key, dirty = key, False
                 if len(ticks) >= self.run_ahead:  # bound how far the host runs ahead of the GPU

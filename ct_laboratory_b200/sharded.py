@@ -64,8 +64,12 @@ def _slice_module(m, lo, hi):
         tv = (m.tvals_uint16[lo:hi], m.tvals_start[lo:hi], m.tvals_scale[lo:hi])
     elif m.tvals_full is not None:
         tv = m.tvals_full[lo:hi]
+    # the fixed-point adjoint carries over to a slice; the gather needs the
+    # whole scan's panel table, so a slice of a gathering module scatters
+    fixed = getattr(m, "adjoint_mode", "atomic") == "fixed"
     return CTProjector3DModule(m.n_x, m.n_y, m.n_z, m.M, m.b, m.src[lo:hi], m.dst[lo:hi], backend=m.backend,
-                               device=m.src.device, tvals=tv, use_compression=m.use_compression, ray_tiling=tiling)
+                               device=m.src.device, tvals=tv, use_compression=m.use_compression, ray_tiling=tiling,
+                               deterministic_adjoint="fixed" if fixed else False)
 
 
 class _Sharded(torch.autograd.Function):

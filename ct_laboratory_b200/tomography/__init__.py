@@ -14,5 +14,6 @@ from .conebeam_projector_3d import *  # noqa: F401,F403
 from .staticct_projector_2d import *  # noqa: F401,F403
 from .staticct_projector_3d import *  # noqa: F401,F403
 from .gather import *  # noqa: F401,F403
+from .fixed_adjoint import *  # noqa: F401,F403
 from .ct_projector_3d_subsets import *  # noqa: F401,F403
 from .ct_projector_3d_multirot import *  # noqa: F401,F403

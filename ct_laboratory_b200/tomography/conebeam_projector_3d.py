@@ -45,7 +45,7 @@ class ConeBeam3DProjector(CTProjector3DModule):
         M, b = standard_image_transform_3d(n_x=n_x, n_y=n_y, n_z=n_z, s_x=voxel_size, s_y=voxel_size,
                                            s_z=voxel_size)
         panels = None
-        if deterministic_adjoint:
+        if deterministic_adjoint == "gather":
             panels = panels_from_grid(src, dst, [v * det_nx * det_ny for v in range(n_view)], det_nx, det_ny, 1,
                                       det_nx, device=device)
         super().__init__(n_x=n_x, n_y=n_y, n_z=n_z, M=M.to(device), b=b.to(device), src=src.to(device),

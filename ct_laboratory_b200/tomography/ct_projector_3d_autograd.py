@@ -11,16 +11,19 @@ Differences from the reference, none of which change the arithmetic:
    loop over 65536-ray chunks (reference :70, :141);
  * ``backend`` may be 'cuda' or 'torch'; both run the CUDA kernels (there is
    no CPU implementation);
- * three optional trailing arguments: ``tiling`` (launch options of the
+ * four optional trailing arguments: ``tiling`` (launch options of the
    on-the-fly kernels), ``M_inv`` (a precomputed M^-1 so that modules can
-   skip the per-call inversion) and ``panels`` (a flat-panel table: the
-   backward then gathers deterministically instead of scattering).
+   skip the per-call inversion), ``panels`` (a flat-panel table: the
+   backward then gathers deterministically instead of scattering) and
+   ``fixed_adjoint`` (the backward scatters in 64-bit fixed point:
+   reproducible, same walk as the forward).
 """
 from __future__ import annotations
 
 import torch
 
 from .ct_projector_3d_cuda import back_project_3d_cuda, forward_project_3d_cuda
+from .fixed_adjoint import back_project_3d_fixed_cuda
 from .gather import back_project_3d_gather_cuda
 
 __all__ = ["CTProjector3DFunction"]
@@ -29,7 +32,7 @@ __all__ = ["CTProjector3DFunction"]
 class CTProjector3DFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, volume, t_main, t_start, t_scale, M, b, src, dst, backend="cuda", tiling=None, M_inv=None,
-                panels=None):
+                panels=None, fixed_adjoint=False):
         if backend not in ("cuda", "torch"):
             raise ValueError(f"unknown backend {backend!r}")
         compressed = t_start is not None and t_scale is not None
@@ -39,6 +42,7 @@ class CTProjector3DFunction(torch.autograd.Function):
         ctx.tiling = tiling
         ctx.M_inv = M_inv
         ctx.panels = panels
+        ctx.fixed_adjoint = bool(fixed_adjoint)
         ctx.volume_shape = volume.shape
         ctx.compressed = compressed
         vol = volume.contiguous()
@@ -59,7 +63,9 @@ class CTProjector3DFunction(torch.autograd.Function):
             g = g.unsqueeze(0)
         if ctx.panels is not None and ctx.tvals is None:
             grad = back_project_3d_gather_cuda(g, src, dst, M, b, n_x, n_y, n_z, ctx.panels, M_inv=ctx.M_inv)
+        elif ctx.fixed_adjoint and ctx.tvals is None:
+            grad = back_project_3d_fixed_cuda(g, src, dst, M, b, n_x, n_y, n_z, tiling=ctx.tiling, M_inv=ctx.M_inv)
         else:
             grad = back_project_3d_cuda(g, ctx.tvals, src, dst, M, b, n_x, n_y, n_z, tiling=ctx.tiling,
                                         M_inv=ctx.M_inv)
-        return grad.reshape(shape), None, None, None, None, None, None, None, None, None, None, None
+        return grad.reshape(shape), None, None, None, None, None, None, None, None, None, None, None, None

@@ -16,10 +16,13 @@ Differences, none in results:
    reference module's encoder (compress_tvals_to_uint16 semantics).
  * M^-1 is computed once on the device and cached until M changes.
  * an optional ``ray_tiling`` launch hint (set by the cone-beam class).
- * ``deterministic_adjoint=True`` (with a flat-panel table ``panels``, which
-   the cone-beam and StaticCT classes build) makes ``back_project`` and the
-   autograd backward gather per voxel: bitwise reproducible, the exact
-   transpose of the forward with the crossing voxel rule.
+ * ``deterministic_adjoint`` makes ``back_project`` and the autograd backward
+   of the on-the-fly projector bitwise reproducible.  ``True`` or ``"fixed"``:
+   the forward's own walk (either voxel rule, any ray layout) scattering in
+   64-bit fixed point (back_project_3d_fixed_cuda).  ``"gather"`` (with a
+   flat-panel table ``panels``, which the cone-beam and StaticCT classes
+   build): per-voxel gathering, the exact transpose of the forward with the
+   crossing voxel rule.
 """
 from __future__ import annotations
 
@@ -32,9 +35,21 @@ from ._common import InverseCache, require_cuda, voxel_diag_len
 from .ct_projector_3d_autograd import CTProjector3DFunction
 from .ct_projector_3d_cuda import back_project_3d_cuda, compute_intersections_3d_cuda
 from .ct_projector_3d_torch import compress_tvals_to_uint16, decompress_tvals_from_uint16
+from .fixed_adjoint import back_project_3d_fixed_cuda
 from .gather import back_project_3d_gather_cuda
 
-__all__ = ["CTProjector3DModule", "precompute_tvals_stitched"]
+__all__ = ["CTProjector3DModule", "precompute_tvals_stitched", "adjoint_mode"]
+
+
+def adjoint_mode(deterministic_adjoint) -> str:
+    """'atomic', 'fixed' or 'gather' for a deterministic_adjoint argument."""
+    if deterministic_adjoint in (False, None, "atomic"):
+        return "atomic"
+    if deterministic_adjoint is True or deterministic_adjoint == "fixed":
+        return "fixed"
+    if deterministic_adjoint == "gather":
+        return "gather"
+    raise ValueError(f"deterministic_adjoint must be False, True, 'fixed' or 'gather', got {deterministic_adjoint!r}")
 
 
 def _trim_inf_columns(t: torch.Tensor) -> torch.Tensor:
@@ -66,9 +81,10 @@ class CTProjector3DModule(torch.nn.Module):
         self.register_buffer("src", f32(src))
         self.register_buffer("dst", f32(dst))
         self.panels = panels
-        self.deterministic_adjoint = bool(deterministic_adjoint)
-        if self.deterministic_adjoint and panels is None:
-            raise ValueError("deterministic_adjoint needs a flat-panel table (panels_from_grid)")
+        self.adjoint_mode = adjoint_mode(deterministic_adjoint)
+        self.deterministic_adjoint = self.adjoint_mode != "atomic"
+        if self.adjoint_mode == "gather" and panels is None:
+            raise ValueError("deterministic_adjoint='gather' needs a flat-panel table (panels_from_grid)")
         self.tvals_uint16 = None
         self.tvals_start = None
         self.tvals_scale = None
@@ -107,7 +123,10 @@ class CTProjector3DModule(torch.nn.Module):
         return self
 
     def _panels(self):
-        return self.panels if (self.deterministic_adjoint and self._table()[0] is None) else None
+        return self.panels if (self.adjoint_mode == "gather" and self._table()[0] is None) else None
+
+    def _fixed(self) -> bool:
+        return self.adjoint_mode == "fixed" and self._table()[0] is None
 
     def _table(self):
         if self.tvals_uint16 is not None:
@@ -126,7 +145,7 @@ class CTProjector3DModule(torch.nn.Module):
         self._ensure_table_device(volume.device)
         t_main, t_start, t_scale = self._table()
         return CTProjector3DFunction.apply(volume, t_main, t_start, t_scale, self.M, self.b, self.src, self.dst,
-                                           self.backend, self.ray_tiling, self.M_inv, self._panels())
+                                           self.backend, self.ray_tiling, self.M_inv, self._panels(), self._fixed())
 
     def forward_project(self, volume):
         return self.forward(volume)
@@ -140,6 +159,9 @@ class CTProjector3DModule(torch.nn.Module):
             if self._panels() is not None:
                 return back_project_3d_gather_cuda(sinogram, self.src, self.dst, self.M, self.b, self.n_x, self.n_y,
                                                    self.n_z, self.panels, M_inv=self.M_inv)
+            if self._fixed():
+                return back_project_3d_fixed_cuda(sinogram.contiguous(), self.src, self.dst, self.M, self.b, self.n_x,
+                                                  self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
             return back_project_3d_cuda(sinogram.contiguous(), tv, self.src, self.dst, self.M, self.b, self.n_x,
                                         self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
 

@@ -91,7 +91,8 @@ class StaticCTProjector3D(CTProjector3DModule):
     def __init__(self, n_x, n_y, n_z, M_gantry, b_gantry, source_positions, module_centers, module_orientations,
                  det_nx_per_module, det_ny_per_module, det_spacing_x, det_spacing_y, source_module_mask,
                  active_sources, M, b, backend="cuda", device: Optional[torch.device] = None,
-                 precomputed_intersections=False, tvals=None, use_compression=True, ray_tiling=None):
+                 precomputed_intersections=False, tvals=None, use_compression=True, ray_tiling=None,
+                 deterministic_adjoint=False):
         if device is None:
             device = torch.device("cuda" if torch.cuda.is_available() else "cpu")
         src, dst = build_static_3d_geometry(source_positions=source_positions, module_centers=module_centers,
@@ -103,7 +104,8 @@ class StaticCTProjector3D(CTProjector3DModule):
                                             device=device)
         super().__init__(n_x=n_x, n_y=n_y, n_z=n_z, M=M.to(device), b=b.to(device), src=src, dst=dst,
                          backend=backend, device=device, precomputed_intersections=precomputed_intersections,
-                         tvals=tvals, use_compression=use_compression, ray_tiling=ray_tiling)
+                         tvals=tvals, use_compression=use_compression, ray_tiling=ray_tiling,
+                         deterministic_adjoint=deterministic_adjoint)
         self.M_gantry, self.b_gantry = M_gantry, b_gantry
         self.source_positions, self.module_centers, self.module_orientations = source_positions, module_centers, \
             module_orientations
@@ -167,7 +169,7 @@ class UniformStaticCTProjector3D(StaticCTProjector3D):
                  det_nx_per_module, det_ny_per_module, det_spacing_x, det_spacing_y, module_z_offset, M_gantry,
                  b_gantry, active_sources, modules_per_source, M, b, backend="cuda", precomputed_intersections=False,
                  tvals=None, use_compression=True, device: Optional[torch.device] = None, ray_tiling=None,
-                 voxel_rule=0):
+                 voxel_rule=0, deterministic_adjoint=False):
         """voxel_rule 0 is the reference's midpoint rule, 1 the crossing
         rule; either way the rays are tiled for the column walk
         (staticct_ray_tiling) unless a ray_tiling is given."""
@@ -189,4 +191,5 @@ class UniformStaticCTProjector3D(StaticCTProjector3D):
                          det_spacing_x=det_spacing_x, det_spacing_y=det_spacing_y, source_module_mask=smm,
                          active_sources=active_sources.to(device), M=M.to(device), b=b.to(device), backend=backend,
                          precomputed_intersections=precomputed_intersections, tvals=tvals,
-                         use_compression=use_compression, device=device, ray_tiling=ray_tiling)
+                         use_compression=use_compression, device=device, ray_tiling=ray_tiling,
+                         deterministic_adjoint=deterministic_adjoint)

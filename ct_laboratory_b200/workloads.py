@@ -250,7 +250,7 @@ class StaticRingWorkload:
         p = self.projector(torch.device("cpu"))
         return p.src, p.dst, p.M, p.b
 
-    def projector(self, device, voxel_rule=0):
+    def projector(self, device, voxel_rule=0, deterministic_adjoint=False):
         import math
 
         import torch
@@ -268,7 +268,7 @@ class StaticRingWorkload:
         return UniformStaticCTProjector3D(*self.n, self.n_source, self.source_radius, 0.0, self.n_module,
                                           self.module_radius, self.det_nx, self.det_ny, self.pitch_x, self.pitch_y,
                                           0.0, Mg, bg, act, self.modules_per_source, M, b, device=device,
-                                          voxel_rule=voxel_rule)
+                                          voxel_rule=voxel_rule, deterministic_adjoint=deterministic_adjoint)
 
     def phantom(self, device="cpu"):
         from .phantoms import ellipsoid_phantom_3d

@@ -168,6 +168,26 @@ int ctlab_back_project_3d_gather_ws(const float* sino, int64_t batch, int64_t n_
                                     int64_t n_y, int64_t n_z, const ctlab_panel* panels, int64_t n_panel, float* out,
                                     void* ray_table, void* stream);
 
+/* Reproducible scatter adjoint: the walk of ctlab_back_project_3d_on_the_fly_ex
+ * (same rays, voxels and segment lengths under either voxel rule) with every
+ * contribution y * len rounded once to a multiple of 2^-e and added as a
+ * 64-bit integer.  Integer addition is associative, so the volume is the same
+ * bits on every run, whatever the launch order or what else shares the GPU.
+ * e is chosen per sinogram from max|y| * (the grid's longest world-space
+ * diagonal) * n_ray <= 2^61, a bound on every voxel's sum; the result differs
+ * from the float scatter by the rounding of n_ray terms, far below the float
+ * adjoint's own order-dependence for any voxel a ray crosses more than a
+ * hair.  A sinogram holding NaN or inf gives a NaN volume.  No counterpart
+ * in the reference (its adjoints scatter with float atomicAdd,
+ * src/ct_projector_3d.cu:1005).  `workspace` is device memory, 256-byte
+ * aligned, of ctlab_back_project_3d_fixed_workspace_bytes bytes (one int64
+ * volume per sinogram plus a header); it is cleared here. */
+int64_t ctlab_back_project_3d_fixed_workspace_bytes(int64_t batch, int64_t n_x, int64_t n_y, int64_t n_z);
+int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int64_t n_ray, const float* src, const float* dst,
+                                const float* M_inv, const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
+                                float* out, int accumulate, const ctlab_ray_opts* tiling, void* workspace,
+                                int64_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* 3-D, precomputed intersections                                          */
 /* ---------------------------------------------------------------------- */

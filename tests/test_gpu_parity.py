@@ -332,11 +332,12 @@ def test_gather_ray_table_one_sinogram(pitch, det):
     assert float(g1.abs().max()) > 0 and rel_err(g1.cpu().numpy(), at.cpu().numpy()) < TOL
 
 
-def test_deterministic_module_backward():
+def test_deterministic_gather_module_backward():
     from ct_laboratory_b200 import ConeBeam3DProjector
     kw = dict(n_x=24, n_y=20, n_z=16, n_view=6, det_nx=32, det_ny=24, sid=100.0, sdd=150.0, det_spacing=0.8,
               voxel_size=0.5, device=torch.device(DEV), voxel_rule=1)
-    p = ConeBeam3DProjector(**kw, deterministic_adjoint=True)
+    p = ConeBeam3DProjector(**kw, deterministic_adjoint="gather")
+    assert p.adjoint_mode == "gather" and p.panels is not None
     q = ConeBeam3DProjector(**kw)
     x = torch.rand(24, 20, 16, device=DEV, requires_grad=True)
     w = torch.rand(p.src.shape[0], device=DEV)

@@ -6,7 +6,9 @@ Tolerance: reconstructions within 1e-4 relative RMSE (the stated MAP bar)
 of the sequential MaximumAPosterioriEstimator run and of the same job
 served alone; the server's iteration is written out instead of autograd and
 its adjoint adds in a different atomic order, so results agree to float
-rounding, not bitwise."""
+rounding, not bitwise -- except with the fixed-point adjoint
+(deterministic_adjoint=True), where a job alone and in the mix agree
+bitwise."""
 import dataclasses
 
 import numpy as np
@@ -89,3 +91,44 @@ def test_srpt_and_all_policies_give_the_same_reconstructions(jobs):
     b = {r["job_id"]: r["x"] for r in ReconServer(DEV, policy="srpt", tick_rays=1).run(jobs)}
     for j in jobs:
         assert rel_rmse(a[j.job_id], b[j.job_id]) <= TOL
+
+
+def test_deterministic_adjoint_alone_and_in_the_mix_bitwise(jobs):
+    """With the fixed-point adjoint a job's reconstruction is the same bits
+    served alone, among the others, and under either scheduling policy; and
+    it stays within the MAP bar of the float-atomic server."""
+    from ct_laboratory_b200.serving import ReconServer
+    mixed = {r["job_id"]: r["x"] for r in ReconServer(DEV, deterministic_adjoint=True).run(jobs)}
+    srpt = {r["job_id"]: r["x"] for r in ReconServer(DEV, deterministic_adjoint=True, policy="srpt",
+                                                      tick_rays=1).run(jobs)}
+    atomic = {r["job_id"]: r["x"] for r in ReconServer(DEV).run(jobs)}
+    for j in jobs:
+        alone = ReconServer(DEV, deterministic_adjoint=True).run([dataclasses.replace(j, arrival_s=0.0)])[0]["x"]
+        assert torch.equal(mixed[j.job_id], alone), j.job_id
+        assert torch.equal(mixed[j.job_id], srpt[j.job_id]), j.job_id
+        assert rel_rmse(mixed[j.job_id], atomic[j.job_id]) <= TOL, j.job_id
+
+
+def test_scan_batch_deterministic_adjoint_is_scan_independent():
+    """ScanBatch(deterministic_adjoint=True): each scan's adjoint is the same
+    bits in any batch and equals the single-scan fixed-point call."""
+    from ct_laboratory_b200 import ConeBeam3DProjector
+    from ct_laboratory_b200.batched import ScanBatch
+    from ct_laboratory_b200.tomography import back_project_3d_fixed_cuda
+    ps = [ConeBeam3DProjector(n, n, n, n_view=v, det_nx=40, det_ny=32, sid=100.0, sdd=150.0, det_spacing=0.8,
+                              voxel_size=0.5, voxel_rule=1, device=DEV) for n, v in ((24, 10), (32, 7), (20, 12))]
+    g = torch.Generator(device=DEV).manual_seed(4)
+    ys = [torch.rand(p.src.shape[0], generator=g, device=DEV) for p in ps]
+    outs = []
+    for sel in ([0, 1, 2], [1], [2, 0]):
+        b = ScanBatch([ps[i] for i in sel], deterministic_adjoint=True)
+        for k, i in enumerate(sel):
+            b.sinos_in[k].copy_(ys[i])
+        b.back()
+        outs.append({i: b.images_out[k].clone() for k, i in enumerate(sel)})
+    for i, p in enumerate(ps):
+        want = back_project_3d_fixed_cuda(ys[i], p.src, p.dst, p.M, p.b, p.n_x, p.n_y, p.n_z, tiling=p.ray_tiling,
+                                          M_inv=p.M_inv)
+        for o in outs:
+            if i in o:
+                assert torch.equal(o[i], want), i
