@@ -60,11 +60,21 @@ __global__ void __launch_bounds__(256) add_transposed_kernel(float* __restrict__
 #ifndef CTLAB_XY_MIN_BLOCKS
 #define CTLAB_XY_MIN_BLOCKS 4
 #endif
+// The midpoint walk's adjoint (one volume) targets 3: with up to 85
+// registers a thread it measured 8.91 ms on the cone256 scan against 9.31
+// at 4 (64 registers), while its forward and the crossing-rule adjoint are
+// faster at 4 (9.67 against 10.71 ms; 8.43 against 8.53 ms).
+#ifndef CTLAB_XY_MIN_BLOCKS_ADJ
+#define CTLAB_XY_MIN_BLOCKS_ADJ CTLAB_XY_MIN_BLOCKS
+#endif
+#ifndef CTLAB_MID_MIN_BLOCKS_ADJ
+#define CTLAB_MID_MIN_BLOCKS_ADJ 3
+#endif
 
 // blockIdx.y covers batch items NB at a time: the walk of a tile is done once
 // for NB volumes (a batch of B volumes costs B / NB walks, not B).
 template <bool ADJ, int NB, int W = 32>
-__global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
+__global__ void __launch_bounds__(256, NB == 1 ? (ADJ ? CTLAB_XY_MIN_BLOCKS_ADJ : CTLAB_XY_MIN_BLOCKS) : 3)
     siddon3d_shared_xy_kernel(const float* __restrict__ in, float* __restrict__ out, const float* __restrict__ src,
                               const float* __restrict__ dst, int64_t n_ray, const float* __restrict__ M_inv,
                               const float* __restrict__ bvec, GridDims<3> G, int64_t nvox, Tiling T, int batch) {
@@ -79,7 +89,7 @@ __global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
 // (shared_xy_ray_mid): per warp the round's crossing parameters and its
 // certified cell records.
 template <bool ADJ, int NB, int W = 32>
-__global__ void __launch_bounds__(256, NB == 1 ? CTLAB_XY_MIN_BLOCKS : 3)
+__global__ void __launch_bounds__(256, NB == 1 ? (ADJ ? CTLAB_MID_MIN_BLOCKS_ADJ : CTLAB_XY_MIN_BLOCKS) : 3)
     siddon3d_shared_xy_mid_kernel(const float* __restrict__ in, float* __restrict__ out,
                                   const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
                                   const float* __restrict__ M_inv, const float* __restrict__ bvec, GridDims<3> G,
@@ -214,7 +224,7 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
 // The column walks (either voxel rule) over one sinogram per blockIdx.y,
 // into its int64 volume.
 template <bool MID, int W>
-__global__ void __launch_bounds__(256, CTLAB_XY_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, MID ? CTLAB_MID_MIN_BLOCKS_ADJ : CTLAB_XY_MIN_BLOCKS_ADJ)
     siddon3d_fixed_column_kernel(const float* __restrict__ in, float* __restrict__ sums,
                                  const float* __restrict__ src, const float* __restrict__ dst, int64_t n_ray,
                                  const float* __restrict__ M_inv, const float* __restrict__ bvec, GridDims<3> G,

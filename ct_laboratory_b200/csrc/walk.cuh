@@ -82,6 +82,25 @@ __device__ __forceinline__ int midpoint_voxel(const AffineT<NDIM>& A, const floa
     return ok ? flat : -1;
 }
 
+// midpoint_voxel for a diagonal M^-1 (every off-diagonal entry zero): each
+// index from its own axis, i_a = rne(m_aa (fma(tm, v_a, s_a) - b_a)).
+// world_to_index3 adds only exact zeros to these products (0 * x = +-0, and
+// x + +-0 = x for x != 0; a zero sum rounds to index 0 either way), so the
+// voxel is the same as midpoint_voxel's.
+__device__ __forceinline__ int midpoint_voxel_diag(const Affine3& A, const float* sw, const float* vw, float t0,
+                                                   float t1, const GridDims<3>& G) {
+    const float tm = __fmul_rn(0.5f, __fadd_rn(t0, t1));
+    int flat = 0;
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int i = rne_int(__fmul_rn(A.m[4 * a], __fsub_rn(__fmaf_rn(tm, vw[a], sw[a]), A.b[a])));
+        ok = ok && (unsigned)i < (unsigned)G.n[a];
+        flat += i * G.stride[a];
+    }
+    return ok ? flat : -1;
+}
+
 // Segments next to the grid under the midpoint rule.  The reference forms a
 // segment between every two consecutive plane hits in [0, 1] (the end points
 // 0 and 1 included, ct_projector_3d.cu:889-891) and charges it to the voxel
@@ -92,13 +111,14 @@ __device__ __forceinline__ int midpoint_voxel(const AffineT<NDIM>& A, const floa
 // reference forms next to the entry (DIR = -1, from t_edge = t_enter
 // backwards) or the exit (DIR = +1, from t_edge = t_exit onwards): the
 // neighbouring hits are the next in-range plane of each axis beyond the
-// edge, or the end point.  It records up to kEdge of them, nearest first,
+// edge, or the end point (DIAG: M^-1 is diagonal, midpoint_voxel_diag).
+// It records up to kEdge of them, nearest first,
 // and stops at the first whose midpoint rounds outside the grid.  p0[a] is a
 // plane of axis a at or beyond the edge (its parameter on the far side of
 // t_edge or equal to it).
 constexpr int kEdge = 2;
 
-template <int NDIM, int DIR>
+template <int NDIM, int DIR, bool DIAG = false>
 __device__ __forceinline__ int edge_segments(const AffineT<NDIM>& A, const float* sw, const float* vw,
                                              const float* s, const float* inv, const float* ps, const float* p0,
                                              float t_edge, float ray_len, const GridDims<NDIM>& G, int* vox,
@@ -134,7 +154,9 @@ __device__ __forceinline__ int edge_segments(const AffineT<NDIM>& A, const float
 #pragma unroll
         for (int a = 0; a < NDIM; ++a) t_far = DIR > 0 ? fminf(t_far, tq[a]) : fmaxf(t_far, tq[a]);
         const float lo = DIR > 0 ? t_near : t_far, hi = DIR > 0 ? t_far : t_near;
-        const int m = midpoint_voxel<NDIM>(A, sw, vw, lo, hi, G);
+        int m;
+        if constexpr (DIAG && NDIM == 3) m = midpoint_voxel_diag(A, sw, vw, lo, hi, G);
+        else m = midpoint_voxel<NDIM>(A, sw, vw, lo, hi, G);
         if (m < 0) break;
         vox[n] = m;
         len[n] = __fmul_rn(__fsub_rn(hi, lo), ray_len);
@@ -1339,9 +1361,12 @@ __device__ __forceinline__ int count_le(const float* v, float key) {
     return c + (v[c] <= key ? 1 : 0);
 }
 
-// Cells per pass-1 step (forward: gathers in flight per lane).
+// Cells per pass-1 step (forward: gathers in flight per lane).  On the
+// cone256 scan the forward measured 9.67 ms with 4 against 9.77 with 8 and
+// 10.04 with 16; the adjoint 9.33 ms with 4 against 9.52 with 2 and 9.94
+// with 8.
 #ifndef CTLAB_MID_GROUP_FWD
-#define CTLAB_MID_GROUP_FWD 8
+#define CTLAB_MID_GROUP_FWD 4
 #endif
 #ifndef CTLAB_MID_GROUP_ADJ
 #define CTLAB_MID_GROUP_ADJ 4
@@ -1500,7 +1525,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         float p0[3], ps[3], el[kEdge];
         int ev[kEdge];
         edge_planes<-1>(R, t_enter, G, p0, ps);
-        const int ne = edge_segments<3, -1>(A, sw, vw, R.s, R.inv, ps, p0, t_enter, 1.f, G, ev, el);
+        const int ne = edge_segments<3, -1, true>(A, sw, vw, R.s, R.inv, ps, p0, t_enter, 1.f, G, ev, el);
 #pragma unroll
         for (int k = kEdge - 1; k >= 0; --k) charge(ev[k], el[k], k < ne && el[k] > 0.f);
     }
@@ -1559,8 +1584,10 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
                     const int k = k_at(c.tm);
                     bool use = c.col >= 0 && (unsigned)k < nz;
                     if (!UNI) use = use && p0 >= t_enter && c.t <= t_exit;
-                    vq[u] = use ? c.col + k : 0;
-                    wq[u] = use ? c.span : 0.f;  // (an unused cell's span may be inf - inf)
+                    // index and span are read only where `use` holds (an unused
+                    // cell's span may be inf - inf; no select is spent on it)
+                    vq[u] = (int)((unsigned)c.col + (unsigned)k);
+                    wq[u] = c.span;
                     uq[u] = use;
                     p0 = c.t;
                 }
@@ -1604,7 +1631,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
                             const bool zin = tnz < hi;
                             const float e = zin ? tnz : hi;
                             if (e > t) {
-                                const int v = midpoint_voxel<3>(A, sw, vw, t, e, G);
+                                const int v = midpoint_voxel_diag(A, sw, vw, t, e, G);
                                 charge(v, __fsub_rn(e, t), v >= 0);
                                 t = e;
                             }
@@ -1651,7 +1678,7 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
         float p0[3], ps[3], el[kEdge];
         int ev[kEdge];
         edge_planes<1>(R, t_exit, G, p0, ps);
-        const int ne = edge_segments<3, 1>(A, sw, vw, R.s, R.inv, ps, p0, t_exit, 1.f, G, ev, el);
+        const int ne = edge_segments<3, 1, true>(A, sw, vw, R.s, R.inv, ps, p0, t_exit, 1.f, G, ev, el);
 #pragma unroll
         for (int k = 0; k < kEdge; ++k) charge(ev[k], el[k], k < ne && el[k] > 0.f);
     }
