@@ -392,7 +392,7 @@ def run_ours(args, world, rank, local):
         kern[name] = {"ms_mean": ms, "ms_min": float(t.min()), "achieved_gbs": ach,
                       "frac": (ach / peak) if ach else None}
     dom = max(kern, key=lambda k: kern[k]["ms_mean"])
-    traffic = load_traffic(w.name, dom)
+    traffic = load_traffic(w.name, dom, args.voxel_rule)
     roofline = {"bound": "hbm", "achieved": kern[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
                 "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "segments": seg, "kernels": kern}
@@ -719,14 +719,15 @@ def run_map(args, dev, proj, x_true, y_rand):
     return out
 
 
-def load_traffic(workload, kernel):
-    """DRAM bytes per launch from the committed ncu summary, if any."""
+def load_traffic(workload, kernel, voxel_rule=0):
+    """DRAM bytes per launch from the committed ncu summary, if any (keyed
+    by workload, and "<workload>/crossing" for the crossing voxel rule)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get(workload, {}).get(kernel)
+    return d.get(workload if voxel_rule == 0 else f"{workload}/crossing", {}).get(kernel)
 
 
 def main():

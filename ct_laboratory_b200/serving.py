@@ -115,12 +115,21 @@ def make_jobs(workload, device, lr_scale=1.0):
             y = torch.poisson(spec.I0 * torch.exp(-line), generator=g)
             row = float(p.forward_project(torch.ones_like(x)).max())
             col = float(p.back_project(torch.ones_like(line)).max())
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            p.back_project(p.forward_project(x))
-            e1.record()
-            e1.synchronize()
+            # one forward + adjoint pair as an iteration runs it: the adjoint
+            # of the first iteration's residual y - I0 exp(-A 0), nonzero on
+            # every ray through the volume (the adjoint skips rays whose input
+            # is zero, so A x of the phantom would time too little work);
+            # the second of two timings
+            r0 = y - spec.I0
+            for _ in range(2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                p.forward_project(x)
+                p.back_project(r0)
+                e1.record()
+                e1.synchronize()
             spec.pair_ms = e0.elapsed_time(e1)
+            del r0
         spec.lr = lr_scale / (spec.I0 * row * col)
         spec.y = y.cpu().pin_memory()
         jobs.append(spec)
