@@ -119,14 +119,26 @@ class RaySharded3DProjector(nn.Module):
 
     # -- collectives -----------------------------------------------------------
     def _gather(self, part):
-        """All shards of the sinogram, in ray order, on every rank.  Shards
-        may differ in length: each is padded to the longest for the gather."""
-        lead = part.shape[:-1]
-        pad = part.new_zeros((*lead, self._max_shard))
-        pad[..., :part.shape[-1]] = part
-        bufs = [torch.empty_like(pad) for _ in range(self.world)]
-        dist.all_gather(bufs, pad.contiguous(), group=self.group)
-        return torch.cat([b[..., :h - l] for b, (l, h) in zip(bufs, self.bounds)], dim=-1)
+        """All shards of the sinogram, in ray order, on every rank: one
+        all_gather_into_tensor into a [world, ..., shard] buffer.  Shards may
+        differ in length: each is then padded to the longest for the gather
+        and the padding cut out after.  With equal shards and a single
+        sinogram the buffer is the ray-ordered sinogram itself (no copy)."""
+        lead = tuple(part.shape[:-1])
+        m = self._max_shard
+        equal = all(h - l == m for l, h in self.bounds)
+        src = part.contiguous() if equal else part.new_zeros((*lead, m))
+        if not equal:
+            src[..., :part.shape[-1]] = part
+        rows = int(torch.Size(lead).numel())
+        buf = part.new_empty(self.world * rows * m)  # flat: every backend concatenates along dim 0
+        dist.all_gather_into_tensor(buf, src.reshape(-1), group=self.group)
+        if equal and rows == 1:
+            return buf.reshape(*lead, self.world * m)
+        buf = buf.reshape(self.world, rows, m)
+        if equal:
+            return buf.permute(1, 0, 2).reshape(*lead, self.world * m)
+        return torch.cat([buf[r, :, :h - l] for r, (l, h) in enumerate(self.bounds)], dim=-1).reshape(*lead, -1)
 
     # -- projector API ------------------------------------------------------------
     def local_sinogram(self, volume):

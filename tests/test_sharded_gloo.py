@@ -65,6 +65,11 @@ def _worker(rank, world, port, q):
         errs.append(float((xr.grad - (w @ A).reshape(shape)).abs().max()))
         local = RaySharded3DProjector(lambda lo, hi: Rows(A, lo, hi, shape), n_ray=n_ray, gather_sinogram=False)
         errs.append(float((local.forward_project(x) - (A @ x.reshape(-1))[local.lo:local.hi]).abs().max()))
+        # equal shards (12 rays over 2 or 3 ranks): the gathered buffer is the sinogram itself
+        A12 = torch.rand(12, 24, generator=g, dtype=torch.float64)
+        p12 = RaySharded3DProjector(lambda lo, hi: Rows(A12, lo, hi, shape), n_ray=12)
+        errs.append(float((p12.forward_project(x) - A12 @ x.reshape(-1)).abs().max()))
+        errs.append(float((p12.forward_project(xb) - xb.reshape(2, -1) @ A12.t()).abs().max()))
         q.put((rank, max(errs)))
     finally:
         dist.destroy_process_group()
