@@ -1372,6 +1372,11 @@ __device__ __forceinline__ int count_le(const float* v, float key) {
 #ifndef CTLAB_MID_GROUP_FWD
 #define CTLAB_MID_GROUP_FWD 4
 #endif
+// The same for 16-lane groups (the StaticCT ring's 16-row modules): 8
+// cells measured 2.46 ms per static512 forward against 2.54 with 4.
+#ifndef CTLAB_MID_GROUP_FWD16
+#define CTLAB_MID_GROUP_FWD16 8
+#endif
 #ifndef CTLAB_MID_GROUP_ADJ
 #define CTLAB_MID_GROUP_ADJ 4
 #endif
@@ -1537,7 +1542,8 @@ __device__ __forceinline__ void shared_xy_ray_mid(const float* __restrict__ in, 
     const float fl = (float)lane;
     const int max_rounds = (G.n[0] + G.n[1] + 2) / W + 2;
     const int max_steps = W + G.n[2] + 4;  // pass-2 cells of a round: at most one per z plane, entry and exit
-    constexpr int kNG = ADJ ? CTLAB_MID_GROUP_ADJ : (CTLAB_MID_GROUP_FWD / NB > 0 ? CTLAB_MID_GROUP_FWD / NB : 1);
+    constexpr int kGF = W == 16 ? CTLAB_MID_GROUP_FWD16 : CTLAB_MID_GROUP_FWD;
+    constexpr int kNG = ADJ ? CTLAB_MID_GROUP_ADJ : (kGF / NB > 0 ? kGF / NB : 1);
     static_assert(W % kNG == 0, "pass-1 steps must tile the round's cells");
     const bool uniform = __all_sync(kFullMask, R.live && R.t_enter == t_start && R.t_exit == t_stop);
     float carry = t_start;  // start of the round's first cell
