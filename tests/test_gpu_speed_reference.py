@@ -14,8 +14,8 @@ the column walk, 128-thread CTAs; L2 flushed before each pass).
 
 Parity is checked on those full-size views with the benchmark's own launch
 shape (the detector tiling of the sampled views) and through the _C entry
-points with no launch hint (layout detected), forward and adjoint, at the
-stated 1e-5; the 16-row StaticCT ring (static512) is checked the same way on
+points with no launch hint (layout detected), forward and adjoint, and the
+reproducible fixed-point adjoint, at the stated 1e-5; the 16-row StaticCT ring (static512) is checked the same way on
 a slice of its views.  The reference's adjoint is called through _C with the
 correct M^-1 (its Python wrapper would invert twice,
 ct_projector_3d_cuda.py:209-210, :319).
@@ -108,6 +108,10 @@ def test_cone256_speed_and_parity_vs_reference_cuda(ref):
         f = _C.forward_project_3d_on_the_fly_cuda(x, src, dst, Mi, b, tiling=t)
         a = _C.back_project_3d_on_the_fly_cuda(ys, src, dst, Mi, b, *w.n, tiling=t)
         errs[name] = (rel_err(f.cpu().numpy(), rf), rel_err(a.cpu().numpy(), rb))
+    # the reproducible (fixed-point) adjoint on the same views and launch shape
+    from ct_laboratory_b200.tomography import back_project_3d_fixed_cuda
+    fx = back_project_3d_fixed_cuda(ys, src, dst, proj.M, b, *w.n, tiling=til, M_inv=Mi)
+    errs["fixed_adjoint"] = (0.0, rel_err(fx.cpu().numpy(), rb.reshape(fx.shape)))
     e_f = max(e[0] for e in errs.values())
     e_b = max(e[1] for e in errs.values())
 
@@ -150,3 +154,7 @@ def test_static512_column16_parity_vs_reference_cuda(ref):
         a = _C.back_project_3d_on_the_fly_cuda(y, src, dst, Mi, b, *w.n, tiling=t)
         assert rel_err(f.cpu().numpy(), rf) < 1e-5
         assert rel_err(a.cpu().numpy(), rb) < 1e-5
+    # the reproducible (fixed-point) adjoint, 16-lane column walk
+    from ct_laboratory_b200.tomography import back_project_3d_fixed_cuda
+    fx = back_project_3d_fixed_cuda(y, src, dst, p.M, b, *w.n, tiling=til, M_inv=Mi)
+    assert rel_err(fx.cpu().numpy(), rb.reshape(fx.shape)) < 1e-5
