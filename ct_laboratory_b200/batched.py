@@ -129,7 +129,7 @@ def _cost(p):
 
 class ScanBatch:
     def __init__(self, projectors, voxel_rule=N.VOXEL_CROSSING, forward=True, adjoint=True, block_threads=256,
-                 kind="auto", buffers=None, deterministic_adjoint=False):
+                 kind="auto", buffers=None, deterministic_adjoint=False, fixed_workspace=None):
         self.projectors = list(projectors)
         if not self.projectors:
             raise ValueError("ScanBatch needs at least one projector")
@@ -152,7 +152,14 @@ class ScanBatch:
             if self.ndim != 3:
                 raise ValueError("ScanBatch: deterministic_adjoint is implemented for 3-D scans")
             need = max(int(N.lib.ctlab_back_project_3d_fixed_workspace_bytes(1, *_dims(p))) for p in self.projectors)
-            self._fixed_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+            if fixed_workspace is not None:  # a caller-owned buffer, reused from batch to batch
+                if (fixed_workspace.dtype != torch.uint8 or fixed_workspace.device != self.device
+                        or fixed_workspace.numel() < need):
+                    raise ValueError(f"ScanBatch: fixed_workspace must be a uint8 tensor of >= {need} bytes on "
+                                     f"{self.device}")
+                self._fixed_ws = fixed_workspace
+            else:
+                self._fixed_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
         shapes = [_dims(p) for p in self.projectors]
         n_rays = [int(p.src.shape[0]) for p in self.projectors]
         if buffers is None:

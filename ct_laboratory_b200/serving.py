@@ -88,11 +88,14 @@ class JobSpec:
                                    build_on_device=True)
 
 
-def job_bytes(spec):
+def job_bytes(spec, deterministic_adjoint=False):
     """Device footprint of an admitted job: rays (src, dst: 24 B), sinograms
     (y, A x, residual: 12 B) per ray; volumes (estimate, gradient and the
-    prior's temporaries: 16 B) per voxel."""
-    return 36 * spec.n_ray + 16 * spec.n ** 3
+    prior's temporaries: 16 B) per voxel; with the fixed-point adjoint also
+    its int64 sums (8 B per voxel: the server's one shared workspace is
+    sized for the largest job, counted here for every job, an upper
+    bound)."""
+    return 36 * spec.n_ray + (24 if deterministic_adjoint else 16) * spec.n ** 3
 
 
 def make_jobs(workload, device, lr_scale=1.0):
@@ -141,7 +144,7 @@ def make_jobs(workload, device, lr_scale=1.0):
 class _Active:
     """Device state of an admitted job."""
 
-    def __init__(self, spec, device):
+    def __init__(self, spec, device, deterministic_adjoint=False):
         self.spec = spec
         self.proj = spec.projector(device)
         self.y = spec.y.to(device, non_blocking=True)
@@ -151,7 +154,7 @@ class _Active:
         self.p = torch.empty(spec.n_ray, dtype=torch.float32, device=device)
         self.r = torch.empty_like(self.p)
         self.it = 0
-        self.nbytes = job_bytes(spec)
+        self.nbytes = job_bytes(spec, deterministic_adjoint)
 
 
 def _residual_(job):
@@ -214,6 +217,7 @@ class ReconServer:
         active, finishing, results = [], [], {}
         used = 0
         batch, dirty, batch_key = None, True, None
+        det, fixed_ws = self.deterministic_adjoint, None
         ticks = deque()
         n_ticks = peak = 0
         marks = []  # per tick: events before / after the projector and elementwise phases
@@ -227,9 +231,9 @@ class ReconServer:
                         results[jid].update(finish_s=time.perf_counter() - t0, x=host)
                         finishing.remove(f)
                 while (queue and queue[0].arrival_s <= now and len(active) < self.max_active
-                       and used + job_bytes(queue[0]) <= self.budget):
+                       and used + job_bytes(queue[0], det) <= self.budget):
                     s = queue.popleft()
-                    a = _Active(s, dev)
+                    a = _Active(s, dev, det)
                     used += a.nbytes
                     active.append(a)
                     peak = max(peak, len(active))
@@ -239,9 +243,9 @@ class ReconServer:
                 if queue and not active and queue[0].arrival_s > now:
                     time.sleep(min(queue[0].arrival_s - now, 0.002))
                     continue
-                if queue and not active and used + job_bytes(queue[0]) > self.budget and not finishing:
-                    raise RuntimeError(f"job {queue[0].job_id} needs {job_bytes(queue[0])} bytes, more than the "
-                                       f"HBM budget {self.budget}")
+                if queue and not active and used + job_bytes(queue[0], det) > self.budget and not finishing:
+                    raise RuntimeError(f"job {queue[0].job_id} needs {job_bytes(queue[0], det)} bytes, more than "
+                                       f"the HBM budget {self.budget}")
                 if not active:
                     if finishing:
                         torch.cuda.synchronize(dev)
@@ -249,8 +253,14 @@ class ReconServer:
                 sel = self._select(active)
                 key = tuple(id(a) for a in sel)
                 if dirty or key != batch_key:
+                    if det:  # one int64 workspace for every batch, grown to the largest job
+                        need = max(int(N.lib.ctlab_back_project_3d_fixed_workspace_bytes(1, *[a.spec.n] * 3))
+                                   for a in sel)
+                        if fixed_ws is None or fixed_ws.numel() < need:
+                            fixed_ws = None
+                            fixed_ws = torch.empty(need, dtype=torch.uint8, device=dev)
                     batch = ScanBatch([a.proj for a in sel], voxel_rule=N.VOXEL_CROSSING,
-                                      deterministic_adjoint=self.deterministic_adjoint, buffers={"images_in": [a.x for a in sel], "sinos_out": [a.p for a in sel],
+                                      deterministic_adjoint=det, fixed_workspace=fixed_ws, buffers={"images_in": [a.x for a in sel], "sinos_out": [a.p for a in sel],
                                                "sinos_in": [a.r for a in sel], "images_out": [a.g for a in sel]})
                     batch_key, dirty = key, False
                 if len(ticks) >= self.run_ahead:  # bound how far the host runs ahead of the GPU

@@ -18,6 +18,8 @@ def test_serving_workload_is_seeded_and_in_range():
 def test_job_footprint_and_latency_summary():
     s = JobSpec(**WORKLOADS["serve"].jobs()[0])
     assert job_bytes(s) == 36 * s.n_ray + 16 * s.n ** 3
+    # the fixed-point adjoint's int64 sums count 8 B more per voxel
+    assert job_bytes(s, deterministic_adjoint=True) == 36 * s.n_ray + 24 * s.n ** 3
     summ = latency_summary([{"latency_s": 1.0, "arrival_s": 0.0, "finish_s": 1.0},
                             {"latency_s": 3.0, "arrival_s": 1.0, "finish_s": 4.0}])
     assert summ["jobs"] == 2 and abs(summ["jobs_per_s"] - 0.5) < 1e-12 and summ["p50_s"] == 2.0
