@@ -76,7 +76,9 @@ class MaximumAPosterioriEstimator:
         (grad,) = torch.autograd.grad(terms[0], x)
         with torch.no_grad():
             P = self.preconditioner
-            direction = P(P(grad.reshape(-1))).reshape(grad.shape)
+            twice = getattr(P, "twice", None)
+            g = grad.reshape(-1)
+            direction = (twice(g) if twice is not None else P(P(g))).reshape(grad.shape)
             self._x = x.detach().add_(direction, alpha=-self.learning_rate())
         self.steps_taken += 1
         return torch.stack([t.detach() for t in terms])

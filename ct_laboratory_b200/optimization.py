@@ -36,6 +36,11 @@ class Preconditioner(nn.Module):
     def inverse(self, x):  # pragma: no cover - overridden by every concrete class
         raise NotImplementedError
 
+    def twice(self, x):
+        """P(P(x)), the MAP estimator's step direction from a gradient; a
+        subclass may give it in one pass."""
+        return self(self(x))
+
 
 class IdentityPreconditioner(Preconditioner):
     """P = I."""

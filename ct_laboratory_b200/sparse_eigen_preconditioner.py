@@ -159,8 +159,9 @@ def thick_restart_lanczos(dec, gram, N, k, tol=1e-3, ncv=None, max_restarts=50, 
     """k largest eigenpairs by thick-restart Lanczos, on the device.
 
     Basis V ((ncv+1) x N, one vector per row, so that every product with it
-    reads whole contiguous vectors) in float32 with two passes of classical
-    Gram-Schmidt against all previous vectors per step; the projected matrix
+    reads whole contiguous vectors) in float32 with classical Gram-Schmidt
+    against all previous vectors per step, a second pass where the first
+    removed most of the new vector (the DGKS test); the projected matrix
     T = V G V^T in float64.  After ncv vectors the k leading Ritz vectors and
     the residual direction are kept and the iteration continues from them.
     Converged when every kept Ritz pair has residual |beta s_last| <= tol
@@ -179,11 +180,17 @@ def thick_restart_lanczos(dec, gram, N, k, tol=1e-3, ncv=None, max_restarts=50, 
     for restart in range(int(max_restarts)):
         for j in range(start, ncv):
             w = dec._gram.vector(V[j])
+            norm_in = w.norm()
             h = V[:j + 1] @ w
             w = w - V[:j + 1].t() @ h
-            h2 = V[:j + 1] @ w
-            w = w - V[:j + 1].t() @ h2
-            h = (h + h2).double()
+            # a second classical Gram-Schmidt pass where the first removed
+            # most of w (|w| fell below 1/sqrt(2) of its norm: the Daniel-
+            # Gragg-Kaufman-Stewart test), else the first pass is enough
+            if bool(w.norm() < 0.7071 * norm_in):
+                h2 = V[:j + 1] @ w
+                w = w - V[:j + 1].t() @ h2
+                h = h + h2
+            h = h.double()
             T[:j + 1, j] = h
             T[j, :j + 1] = h
             beta = w.norm()
@@ -393,6 +400,15 @@ class SparseEigenImagePreconditioner(_LowRankPreconditioner):
 
     def _low_rank(self, x, g):
         return torch.mv(self.rows.t(), torch.mv(self.rows, x) * g)
+
+    def twice(self, x):
+        """P(P(x)) in one pass over the basis.  With orthonormal rows
+        (V^T V = I: eigenvectors) P = V diag(g) V^T + f I gives
+        P^2 = V diag(g^2 + 2 f g) V^T + f^2 I, equal to P(P(x)) up to
+        rounding and to the rows' departure from orthonormality."""
+        xf = x.reshape(-1)
+        g, f = self.gains[0], self.floor[0]
+        return torch.mv(self.rows.t(), torch.mv(self.rows, xf) * (g * g + 2.0 * f * g)) + (f * f) * xf
 
 
 class SparseEigenProjectionPreconditioner(_LowRankPreconditioner):
