@@ -451,13 +451,24 @@ def run_e2e(proj, x, y, args, dev, w, world=1, rays_per_step=None):
     (PCIe is full duplex, and the GPU has a copy engine per direction), so
     step i+1's inputs upload while step i computes and step i's results
     download under step i+1; the timed region ends when every copy of the
-    last step has landed."""
+    last step has landed.
+
+    Ray-sharded (one scan over the ranks): every rank uploads the volume and
+    its own shard of the adjoint input, and downloads its own shard of the
+    all-gathered sinogram; rank 0 downloads the summed back-projection.  So
+    the job's sinograms cross the host links once in all, while the device
+    work is what the device-timed value measures."""
+    import torch.distributed as dist
+    sharded = bool(getattr(args, "sharded", False)) and hasattr(proj, "lo")
+    rank = dist.get_rank() if (sharded and dist.is_initialized()) else 0
+    lo, hi = (proj.lo, proj.hi) if sharded else (0, y.numel())
     x_h = x.cpu().pin_memory()
-    y_h = y.cpu().pin_memory()
-    sino_h = torch.empty(y.shape, dtype=torch.float32).pin_memory()
-    vol_h = torch.empty(x.shape, dtype=torch.float32).pin_memory()
+    y_h = y[lo:hi].cpu().pin_memory()
+    sino_h = torch.empty(hi - lo, dtype=torch.float32).pin_memory()
+    get_vol = rank == 0 or not sharded
+    vol_h = torch.empty(x.shape if get_vol else (0,), dtype=torch.float32).pin_memory()
     xd = [torch.empty_like(x) for _ in range(2)]
-    yd = [torch.empty_like(y) for _ in range(2)]
+    yd = [torch.empty(hi - lo, dtype=y.dtype, device=y.device) for _ in range(2)]
     stream = torch.cuda.current_stream(dev)
     h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     done = [None, None]  # compute of the step that last used buffer set k
@@ -482,10 +493,11 @@ def run_e2e(proj, x, y, args, dev, w, world=1, rays_per_step=None):
         done[k] = ev_b
         with torch.cuda.stream(d2h):
             d2h.wait_event(ev_f)
-            sino_h.copy_(s, non_blocking=True)
+            sino_h.copy_(s.reshape(-1)[lo:hi], non_blocking=True)
             s.record_stream(d2h)
             d2h.wait_event(ev_b)
-            vol_h.copy_(v, non_blocking=True)
+            if get_vol:
+                vol_h.copy_(v, non_blocking=True)
             v.record_stream(d2h)
 
     with torch.no_grad():
@@ -505,9 +517,14 @@ def run_e2e(proj, x, y, args, dev, w, world=1, rays_per_step=None):
     ms = max_over_ranks(e0.elapsed_time(e1), world) / args.e2e_steps
     n_ray = y.numel()
     rays = world * n_ray if rays_per_step is None else rays_per_step
+    if sharded:  # the job's bytes: every rank's volume upload, one sinogram each way, one volume back
+        h2d = world * x_h.numel() * 4 + n_ray * 4
+        d2h = n_ray * 4 + x.numel() * 4
+    else:
+        h2d = world * (x_h.numel() * 4 + y_h.numel() * 4)
+        d2h = world * (sino_h.numel() * 4 + vol_h.numel() * 4)
     return {"value": rays / (ms / 1e3) / 1e9, "unit": "GRays/s", "ms_per_step": ms,
-            "h2d_bytes_per_step": int(world * (x_h.numel() * 4 + y_h.numel() * 4)),
-            "d2h_bytes_per_step": int(world * (sino_h.numel() * 4 + vol_h.numel() * 4)),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "api": f"{type(proj).__name__}.__call__ + .back_project" +
                    ", inputs double-buffered, H2D and D2H each on a stream of its own"}
 
