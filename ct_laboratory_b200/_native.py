@@ -94,6 +94,8 @@ _SIGS = {
     "ctlab_batch_default_ctas": [_I32, _I, _I, _I32, ctypes.POINTER(_I32)],
     "ctlab_project_batched_noalloc": [_SP, _I32, _I, _I, _I32, _I32, _P],
     "ctlab_back_project_3d_fixed": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P, _I64, _P],
+    "ctlab_map_poisson_residual": [_P, _P, _P, _I64, _F, _P],
+    "ctlab_map_smoothness_step": [_P, _P, _I64, _I64, _I64, _F, _F, _P],
 }
 
 for _name, _args in _SIGS.items():

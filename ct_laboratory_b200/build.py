@@ -21,7 +21,7 @@ LIB_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIB_DIR, "libctlab_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["capi.cu", "siddon.cu", "tvals.cu", "gather.cu", "batched.cu"]
+SOURCES = ["capi.cu", "siddon.cu", "tvals.cu", "gather.cu", "batched.cu", "map_step.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

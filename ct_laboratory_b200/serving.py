@@ -158,20 +158,18 @@ class _Active:
 
 
 def _residual_(job):
-    """r = y - I0 exp(-p), in place in job.r (4 elementwise passes, no allocation)."""
-    torch.neg(job.p, out=job.r)
-    job.r.exp_().mul_(-job.spec.I0).add_(job.y)
+    """r = y - I0 exp(-p) into job.r: one pass (ctlab_map_poisson_residual)."""
+    N.call("ctlab_map_poisson_residual", N.ptr(job.y), N.ptr(job.p), N.ptr(job.r), job.p.numel(),
+           float(job.spec.I0), N.stream_of(job.p))
 
 
 def _prior_and_step_(job):
-    """g += w sum_d D_d^T D_d x (non-periodic differences), then x -= lr g."""
-    x, g, w = job.x, job.g, job.spec.prior_w
-    for d in range(3):
-        n = x.shape[d]
-        diff = torch.diff(x, dim=d)
-        g.narrow(d, 0, n - 1).sub_(diff, alpha=w)
-        g.narrow(d, 1, n - 1).add_(diff, alpha=w)
-    x.sub_(g, alpha=job.spec.lr)
+    """g += w sum_d D_d^T D_d x (non-periodic differences), then x -= lr g:
+    one pass for the prior's gradient, one for the step
+    (ctlab_map_smoothness_step)."""
+    n = job.spec.n
+    N.call("ctlab_map_smoothness_step", N.ptr(job.x), N.ptr(job.g), n, n, n, float(job.spec.prior_w),
+           float(job.spec.lr), N.stream_of(job.x))
 
 
 class ReconServer:

@@ -82,14 +82,18 @@ int ctlab_invert_matrix(const float* M, int n, float* M_inv, int* singular, void
 #define CTLAB_VOXEL_MIDPOINT 0
 #define CTLAB_VOXEL_CROSSING 1
 /* Walk: CTLAB_WALK_LANE walks each ray on its own lane.  CTLAB_WALK_COLUMN
- * (3-D, crossing rule, detector-row tilings with tile_rows a multiple of 32,
- * grid dimensions <= 65536) derives the merged x-y crossings of a warp's
- * shared line once per warp and splits each x-y cell per lane at its z
- * planes; warps whose rays do not share their x-y line, or whose z slope is
- * steeper than 3/4 of the x-y slope, fall back to the lane walk inside the
- * same launch.  Both give bitwise equal forward projections.
- * CTLAB_WALK_AUTO takes the column walk wherever it applies (it is the
- * faster one measured) and the lane walk elsewhere. */
+ * (3-D, either voxel rule, detector-row tilings with tile_rows a multiple of
+ * 32 or equal to 16, grid dimensions <= 65536) derives the merged x-y
+ * crossings of a warp's shared line (or of each 16-lane group's) once and
+ * splits each x-y cell per lane at its z planes.  Warps fall back to the
+ * lane walk inside the same launch where their rays do not share their x-y
+ * line; under the crossing rule also where a ray's z slope is steeper than
+ * 3/4 of its x-y slope, and under the midpoint rule where M^-1 is not
+ * diagonal.  The crossing rule's two walks give bitwise equal forward
+ * projections; under the midpoint rule the column walk sums in another
+ * order (equal to rounding).  CTLAB_WALK_AUTO takes the column walk
+ * wherever it applies (the faster one measured) and the lane walk
+ * elsewhere. */
 #define CTLAB_WALK_AUTO 0
 #define CTLAB_WALK_LANE 1
 #define CTLAB_WALK_COLUMN 2
@@ -187,6 +191,23 @@ int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int64_t n_ray,
                                 const float* M_inv, const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
                                 float* out, int accumulate, const ctlab_ray_opts* tiling, void* workspace,
                                 int64_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Elementwise steps of a MAP iteration (the reconstruction server)        */
+/* ---------------------------------------------------------------------- */
+
+/* r[i] = y[i] - I0 exp(-p[i]) for i < n: the Beer-Lambert Poisson residual
+ * of p = A x.  No counterpart in the reference, which forms it through
+ * autograd (probability/random_variables/poisson.py:36-47). */
+int ctlab_map_poisson_residual(const float* y, const float* p, float* r, int64_t n, float I0, void* stream);
+
+/* g += w * sum_d D_d^T D_d x (D_d the forward difference along axis d of the
+ * [n_x][n_y][n_z] volume, no wrap-around), then x -= lr * g: the quadratic
+ * smoothness prior's gradient and the gradient step.  No counterpart in the
+ * reference, which forms it through autograd (image_energies.py:18-29,
+ * bayesian_estimation/map_estimator.py:102-117). */
+int ctlab_map_smoothness_step(float* x, float* g, int64_t n_x, int64_t n_y, int64_t n_z, float w, float lr,
+                              void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* 3-D, precomputed intersections                                          */

@@ -132,3 +132,34 @@ def test_scan_batch_deterministic_adjoint_is_scan_independent():
         for o in outs:
             if i in o:
                 assert torch.equal(o[i], want), i
+
+
+def test_native_map_steps_match_the_written_out_iteration():
+    """ctlab_map_poisson_residual and ctlab_map_smoothness_step against the
+    same iteration written with torch ops (non-periodic differences along
+    every axis, including axes of length 1 and 2), to float rounding."""
+    from ct_laboratory_b200 import _native as N
+    gen = torch.Generator(device=DEV).manual_seed(9)
+    for shape in ((5, 7, 3), (1, 4, 6), (2, 1, 9), (16, 16, 16)):
+        x = torch.rand(shape, generator=gen, device=DEV)
+        grad = torch.rand(shape, generator=gen, device=DEV) - 0.5
+        w, lr = 0.3, 0.05
+        want_g = grad.clone()
+        for d in range(3):
+            n = x.shape[d]
+            if n > 1:
+                diff = torch.diff(x, dim=d)
+                want_g.narrow(d, 0, n - 1).sub_(diff, alpha=w)
+                want_g.narrow(d, 1, n - 1).add_(diff, alpha=w)
+        want_x = x - lr * want_g
+        xx, gg = x.clone(), grad.clone()
+        N.call("ctlab_map_smoothness_step", N.ptr(xx), N.ptr(gg), *shape, w, lr, N.stream_of(xx))
+        assert float((gg - want_g).abs().max()) <= 1e-6 * float(want_g.abs().max()), shape
+        assert float((xx - want_x).abs().max()) <= 1e-6 * float(want_x.abs().max()), shape
+    p = torch.rand(1000, generator=gen, device=DEV) * 3
+    y = torch.poisson(1e4 * torch.exp(-p), generator=gen)
+    r = torch.empty_like(p)
+    N.call("ctlab_map_poisson_residual", N.ptr(y), N.ptr(p), N.ptr(r), p.numel(), 1e4, N.stream_of(p))
+    want = y - 1e4 * torch.exp(-p)
+    # (r is a small difference of numbers near I0: compare at the scale of y)
+    assert float((r - want).abs().max()) <= 1e-6 * float(y.abs().max())
