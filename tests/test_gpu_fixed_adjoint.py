@@ -139,3 +139,39 @@ def test_fixed_module_backward(rule):
     assert torch.equal(g, x.grad)
     assert torch.equal(g, p.back_project(w))
     assert rel_err(g.cpu().numpy(), q.back_project(w).cpu().numpy()) < TOL_FLOAT
+
+
+def test_fixed_adjoint_without_rays_and_host_errors():
+    """No rays: the volume comes out zero (accumulate leaves it as it was);
+    a workspace that is too small or misaligned, a batch outside [1, 65535]
+    and a deterministic 2-D ScanBatch are refused on the host."""
+    from ct_laboratory_b200 import FanBeam2DProjector
+    from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.batched import ScanBatch
+    n = (8, 6, 4)
+    Mi = torch.eye(3, device=DEV).contiguous()
+    b = torch.zeros(3, device=DEV)
+    need = N.lib.ctlab_back_project_3d_fixed_workspace_bytes(1, *n)
+    ws = torch.empty(need + 256, dtype=torch.uint8, device=DEV)
+    out = torch.full((1, *n), 7.0, device=DEV)
+    stream = N.stream_of(out)
+    for acc, want in ((1, 7.0), (0, 0.0)):
+        N.call("ctlab_back_project_3d_fixed", None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), acc,
+               None, N.ptr(ws), need, stream)
+        torch.cuda.synchronize()
+        assert bool((out == want).all())
+    assert N.lib.ctlab_back_project_3d_fixed_workspace_bytes(0, *n) < 0
+    rc = N.lib.ctlab_back_project_3d_fixed(None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
+                                           N.ptr(ws), need - 8, stream)
+    assert rc != 0 and b"workspace" in N.lib.ctlab_last_error()
+    odd = ws[8:]  # 8 bytes past a 256-byte boundary
+    rc = N.lib.ctlab_back_project_3d_fixed(None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
+                                           N.ptr(odd), need, stream)
+    assert rc != 0
+    rc = N.lib.ctlab_back_project_3d_fixed(None, 0, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
+                                           N.ptr(ws), need, stream)
+    assert rc != 0 and b"batch" in N.lib.ctlab_last_error()
+    fan = FanBeam2DProjector(16, 16, n_view=4, n_det=20, sid=100.0, sdd=150.0, det_spacing=1.0, pixel_size=1.0,
+                             device=torch.device(DEV))
+    with pytest.raises(ValueError):
+        ScanBatch([fan], deterministic_adjoint=True)
