@@ -253,9 +253,15 @@ def forward_project_3d_on_the_fly_cuda(volume, src, dst, M_inv, b, tiling=None):
     batch, (n_x, n_y, n_z) = _vol_shape(volume, 3)
     n_ray = src.shape[0]
     out = torch.empty((batch, n_ray), device=volume.device, dtype=torch.float32)
+    act = getattr(tiling, "active", None)  # a list of the active tiles (_native.active_tiling)
     with torch.cuda.device(volume.device):
-        N.call("ctlab_forward_project_3d_on_the_fly_ex", N.ptr(volume), batch, n_x, n_y, n_z, N.ptr(src), N.ptr(dst),
-               n_ray, N.ptr(M_inv), N.ptr(b), N.ptr(out), N.tiling_ref(tiling), N.stream_of(volume))
+        if act is not None:
+            N.call("ctlab_forward_project_3d_on_the_fly_tiles", N.ptr(volume), batch, n_x, n_y, n_z, N.ptr(src),
+                   N.ptr(dst), n_ray, N.ptr(M_inv), N.ptr(b), N.ptr(out), N.tiling_ref(tiling), N.ptr(act[0]),
+                   act[1], N.stream_of(volume))
+        else:
+            N.call("ctlab_forward_project_3d_on_the_fly_ex", N.ptr(volume), batch, n_x, n_y, n_z, N.ptr(src),
+                   N.ptr(dst), n_ray, N.ptr(M_inv), N.ptr(b), N.ptr(out), N.tiling_ref(tiling), N.stream_of(volume))
     return out
 
 
@@ -269,9 +275,15 @@ def back_project_3d_on_the_fly_cuda(sino, src, dst, M_inv, b, n_x, n_y, n_z, til
         tiling = _layout.detect_tiling(src, dst)
     batch, n_ray = _sino_shape(sino)
     out = torch.empty((batch, n_x, n_y, n_z), device=sino.device, dtype=torch.float32)
+    act = getattr(tiling, "active", None)
     with torch.cuda.device(sino.device):
-        N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst),
-               N.ptr(M_inv), N.ptr(b), n_x, n_y, n_z, N.ptr(out), 0, N.tiling_ref(tiling), N.stream_of(sino))
+        if act is not None:
+            N.call("ctlab_back_project_3d_on_the_fly_tiles", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst),
+                   N.ptr(M_inv), N.ptr(b), n_x, n_y, n_z, N.ptr(out), 0, N.tiling_ref(tiling), N.ptr(act[0]), act[1],
+                   N.stream_of(sino))
+        else:
+            N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst),
+                   N.ptr(M_inv), N.ptr(b), n_x, n_y, n_z, N.ptr(out), 0, N.tiling_ref(tiling), N.stream_of(sino))
     return out
 
 

@@ -93,7 +93,13 @@ _SIGS = {
     "ctlab_back_project_batched": [_BP, _I, _I32, _P],
     "ctlab_batch_default_ctas": [_I32, _I, _I, _I32, ctypes.POINTER(_I32)],
     "ctlab_project_batched_noalloc": [_SP, _I32, _I, _I, _I32, _I32, _P],
-    "ctlab_back_project_3d_fixed": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P, _I64, _P],
+    "ctlab_back_project_3d_fixed": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P, _I64, _P,
+                                    _I64, _P],
+    "ctlab_active_tiles": [_P, _P, _I64, _P, _P, _I64, _I64, _I64, _TP, _P, _P, _P, _P],
+    "ctlab_forward_project_3d_on_the_fly_tiles": [_P, _I64, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _TP, _P,
+                                                  _I64, _P],
+    "ctlab_back_project_3d_on_the_fly_tiles": [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64, _P, _I, _TP, _P,
+                                               _I64, _P],
     "ctlab_map_poisson_residual": [_P, _P, _P, _I64, _F, _P],
     "ctlab_map_smoothness_step": [_P, _P, _I64, _I64, _I64, _F, _F, _P],
 }
@@ -109,6 +115,8 @@ lib.ctlab_abi_version.restype = ctypes.c_int
 lib.ctlab_abi_version.argtypes = []
 lib.ctlab_batch_workspace_bytes.restype = ctypes.c_int64
 lib.ctlab_batch_workspace_bytes.argtypes = [_I32]
+lib.ctlab_tile_count.restype = ctypes.c_int64
+lib.ctlab_tile_count.argtypes = [_I64, _TP]
 lib.ctlab_back_project_3d_fixed_workspace_bytes.restype = ctypes.c_int64
 lib.ctlab_back_project_3d_fixed_workspace_bytes.argtypes = [_I64, _I64, _I64, _I64]
 
@@ -118,7 +126,7 @@ ABI_VERSION = lib.ctlab_abi_version()
 def exported_symbols():
     """Names of the C entry points this binding declares."""
     return sorted(_SIGS) + ["ctlab_last_error", "ctlab_abi_version", "ctlab_batch_workspace_bytes",
-                            "ctlab_back_project_3d_fixed_workspace_bytes"]
+                            "ctlab_back_project_3d_fixed_workspace_bytes", "ctlab_tile_count"]
 
 
 def call(name: str, *args) -> None:
@@ -153,3 +161,34 @@ def flat_opts(voxel_rule=VOXEL_MIDPOINT, block_threads=256):
 
 def tiling_ref(t):
     return None if t is None else ctypes.byref(t)
+
+
+class ActiveRayOpts(RayOpts):
+    """RayOpts with the list of the tiling's active tiles (ctlab_active_tiles)
+    as ``active = (int32 CUDA tensor, count)``: the on-the-fly 3-D calls of
+    _C launch only those tiles (the *_tiles entry points)."""
+
+    active = None
+
+
+def active_tiling(t, src, dst, M_inv, b, dims):
+    """An ActiveRayOpts copy of tiling `t` listing the tiles of the scan
+    (src, dst, M_inv, b on one CUDA device; dims = (n_x, n_y, n_z)) that
+    hold a ray the walks charge.  One pass over the rays and one host
+    synchronisation (to read the count)."""
+    n_ray = int(src.shape[0])
+    n_blocks = int(lib.ctlab_tile_count(n_ray, ctypes.byref(t)))
+    if n_blocks < 0:
+        raise RuntimeError(f"ctlab_tile_count failed: {lib.ctlab_last_error().decode(errors='replace')}")
+    dev = src.device
+    flags = torch.empty(n_blocks, dtype=torch.uint8, device=dev)
+    tiles = torch.empty(n_blocks, dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    with torch.cuda.device(dev):
+        call("ctlab_active_tiles", ptr(src), ptr(dst), n_ray, ptr(M_inv), ptr(b), *[int(v) for v in dims],
+             ctypes.byref(t), ptr(flags), ptr(tiles), ptr(count), stream_of(src))
+    n = int(count.item())
+    out = ActiveRayOpts()
+    ctypes.memmove(ctypes.addressof(out), ctypes.addressof(t), ctypes.sizeof(RayOpts))  # copy the fields
+    out.active = (tiles[:n].clone(), n)
+    return out

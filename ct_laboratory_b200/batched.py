@@ -261,8 +261,10 @@ class ScanBatch:
         (the single-scan kernels scan by scan, with the same tile layouts);
         "auto" takes the loop for the 3-D forward, whose single-scan column
         walk is faster than the persistent kernel's on scans of millions of
-        rays (8.75 against 9.98 ms on the cone256 scan), and the persistent
-        launch otherwise.  Returns the forward configuration (the adjoint's
+        rays (8.75 against 9.98 ms on the cone256 scan), and for the 3-D
+        adjoint when every scan has at least 2^20 rays; the persistent launch
+        otherwise.  3-D loop launches take each projector's active-tile
+        list (CTProjector3DModule.active_tiling_for).  Returns the forward configuration (the adjoint's
         is ``config_adj``)."""
         if mode not in ("auto", "persistent", "loop"):
             raise ValueError(f"ScanBatch: mode must be 'auto', 'persistent' or 'loop' (got {mode!r})")
@@ -279,12 +281,23 @@ class ScanBatch:
                     N.call("ctlab_batch_default_ctas", self.ndim, int(d == "adj"), self.voxel_rule,
                            int(block_threads), ctypes.byref(v))
                     ctas = v.value
-            m = mode if mode != "auto" else ("loop" if d == "fwd" and self.ndim == 3 else "persistent")
+            # auto: 3-D scans run one launch each (with their active-tile
+            # lists) where every scan fills the GPU on its own (>= 2^20 rays:
+            # the adjoint of four serving-size scans, 23.6 against 26.1 ms
+            # persistent); the persistent launch otherwise, for batches of
+            # small scans
+            big = all(int(p.src.shape[0]) >= (1 << 20) for p in self.projectors)
+            m = mode if mode != "auto" else (
+                "loop" if self.ndim == 3 and (d == "fwd" or big) else "persistent")
             if d == "adj" and self._fixed_ws is not None:
                 m = "loop"  # the fixed-point adjoint runs scan by scan
             cfg = {"block_threads": int(block_threads), "kind": k, "n_cta": int(ctas), "mode": m}
             opts = [_opts(self.projectors[i], k if isinstance(k, str) else k[i], self.voxel_rule, block_threads)
                     for i in range(len(self.projectors))]
+            if self.ndim == 3 and m == "loop":
+                # the per-scan launches skip each scan's tiles whose rays all
+                # miss its volume (lists cached on the projector)
+                opts = [self.projectors[i].active_tiling_for(o) for i, o in enumerate(opts)]
             if d == "fwd":
                 self.config, self._loop_opts_f = cfg, opts
             else:
@@ -322,7 +335,12 @@ class ScanBatch:
         with torch.cuda.device(self.device):
             for i, p in enumerate(self.projectors):
                 o = self._loop_opts_f[i]
-                if self.ndim == 3:
+                act = getattr(o, "active", None)
+                if self.ndim == 3 and act is not None:
+                    N.call("ctlab_forward_project_3d_on_the_fly_tiles", N.ptr(self.images_in[i]), 1, p.n_x, p.n_y,
+                           p.n_z, N.ptr(p.src), N.ptr(p.dst), int(p.src.shape[0]), N.ptr(p.M_inv), N.ptr(p.b),
+                           N.ptr(self.sinos_out[i]), ctypes.byref(o), N.ptr(act[0]), act[1], st)
+                elif self.ndim == 3:
                     N.call("ctlab_forward_project_3d_on_the_fly_ex", N.ptr(self.images_in[i]), 1, p.n_x, p.n_y,
                            p.n_z, N.ptr(p.src), N.ptr(p.dst), int(p.src.shape[0]), N.ptr(p.M_inv), N.ptr(p.b),
                            N.ptr(self.sinos_out[i]), ctypes.byref(o), st)
@@ -338,11 +356,17 @@ class ScanBatch:
         with torch.cuda.device(self.device):
             for i, p in enumerate(self.projectors):
                 o = self._loop_opts_a[i]
+                act = getattr(o, "active", None)
+                tiles, n_tiles = (N.ptr(act[0]), act[1]) if act is not None else (None, -1)
                 if self._fixed_ws is not None:
                     N.call("ctlab_back_project_3d_fixed", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
-                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), N.ptr(self._fixed_ws),
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), tiles, n_tiles, N.ptr(self._fixed_ws),
                            self._fixed_ws.numel(), st)
+                elif self.ndim == 3 and act is not None:
+                    N.call("ctlab_back_project_3d_on_the_fly_tiles", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
+                           N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,
+                           N.ptr(self.images_out[i]), acc, ctypes.byref(o), tiles, n_tiles, st)
                 elif self.ndim == 3:
                     N.call("ctlab_back_project_3d_on_the_fly_ex", N.ptr(self.sinos_in[i]), 1, int(p.src.shape[0]),
                            N.ptr(p.src), N.ptr(p.dst), N.ptr(p.M_inv), N.ptr(p.b), p.n_x, p.n_y, p.n_z,

@@ -62,6 +62,8 @@ int resolve_tiling(const ctlab_ray_opts* t, int64_t n_ray, Tiling& T) {
     T.tiles_r = (T.n_row + T.tile_rows - 1) / T.tile_rows;
     T.tiles_c = (T.n_col + T.tile_cols - 1) / T.tile_cols;
     T.n_blocks = T.n_view * T.tiles_r * T.tiles_c;
+    T.tiles = nullptr;
+    T.n_full = T.n_blocks;
     return CTLAB_OK;
 }
 

@@ -194,7 +194,9 @@ struct Tiling {
     int64_t view_stride, row_stride, col_stride;
     int tile_rows, tile_cols;       // tile_rows * tile_cols == blockDim.x
     int64_t tiles_r, tiles_c;       // tiles per view along rows / cols
-    int64_t n_blocks;               // n_view * tiles_r * tiles_c
+    int64_t n_blocks;               // tiles launched: n_view * tiles_r * tiles_c, or the list's length
+    const int32_t* tiles = nullptr; // optional list of the tiles to launch (device memory), block b -> tiles[b]
+    int64_t n_full = 0;             // with a list: the tiling's n_view * tiles_r * tiles_c
 };
 
 // Validates `t` (may be NULL = flat) against n_ray and fills `out`.
@@ -226,6 +228,16 @@ __device__ __forceinline__ int64_t tile_ray_at(const Tiling& T, unsigned blk, in
     return view * T.view_stride + row * T.row_stride + col * T.col_stride;
 }
 
-__device__ __forceinline__ int64_t tile_ray(const Tiling& T) { return tile_ray_at(T, blockIdx.x, threadIdx.x); }
+// The tile of this block: blockIdx.x, or its entry of the tile list (an
+// entry outside the tiling gives no ray).
+__device__ __forceinline__ int64_t tile_ray(const Tiling& T) {
+    unsigned blk = blockIdx.x;
+    if (T.tiles != nullptr) {
+        const int32_t t = __ldg(T.tiles + blockIdx.x);
+        if (t < 0 || (int64_t)t >= T.n_full) return -1;
+        blk = (unsigned)t;
+    }
+    return tile_ray_at(T, blk, threadIdx.x);
+}
 
 }  // namespace ctlab

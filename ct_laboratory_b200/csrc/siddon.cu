@@ -139,7 +139,8 @@ static void launch_column_nb(int nb, int rows, dim3 g, int threads, cudaStream_t
 template <int NDIM, bool ADJ>
 static int launch_siddon(const char* what, const float* in, float* out, int64_t batch, const int64_t* dims,
                          const float* src, const float* dst, int64_t n_ray, const float* M_inv, const float* b,
-                         int accumulate, const ctlab_ray_opts* tiling, void* stream, float* scratch = nullptr) {
+                         int accumulate, const ctlab_ray_opts* tiling, void* stream, float* scratch = nullptr,
+                         const int32_t* tiles = nullptr, int64_t n_tiles = -1) {
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535], got %lld", what, (long long)batch);
     CTLAB_REQUIRE(n_ray >= 0, "%s: n_ray must be >= 0", what);
     GridDims<NDIM> G;
@@ -171,6 +172,19 @@ static int launch_siddon(const char* what, const float* in, float* out, int64_t 
     int rc = resolve_tiling(tiling, n_ray, T);
     if (rc) return rc;
     CTLAB_REQUIRE(T.n_blocks <= kMaxGrid, "%s: too many rays for one launch", what);
+    if (n_tiles >= 0) {
+        // only the listed tiles run: the rays of every other tile must be
+        // ones the walks do not charge (ctlab_active_tiles), so the forward
+        // zeroes its output first and the adjoint adds nothing for them
+        CTLAB_REQUIRE(n_tiles <= T.n_blocks, "%s: %lld tiles listed, the tiling has %lld", what,
+                      (long long)n_tiles, (long long)T.n_blocks);
+        CTLAB_REQUIRE(n_tiles == 0 || tiles != nullptr, "%s: null tile list", what);
+        if (!ADJ) CTLAB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)(batch * n_ray), s));
+        if (n_tiles == 0) return CTLAB_OK;
+        T.tiles = tiles;
+        T.n_full = T.n_blocks;
+        T.n_blocks = n_tiles;
+    }
     dim3 grid((unsigned)T.n_blocks, (unsigned)batch);
     const int threads = T.tile_rows * T.tile_cols;
     const bool mid = tiling == nullptr || tiling->voxel_rule == CTLAB_VOXEL_MIDPOINT;
@@ -326,6 +340,69 @@ __global__ void __launch_bounds__(256) fixed_to_float_kernel(const long long* __
     }
 }
 
+// ----------------------------------------------------------------------------
+// Active tiles: the tiles of a tiling holding at least one ray that the walks
+// charge.  Every walk tests a ray with lane_setup's checks (finite end
+// points, a non-degenerate direction, an interval of the box inside [0, 1];
+// traverse applies the same ones) before it charges anything, so the rays
+// of every other tile add nothing and project to 0.
+// ----------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) tile_live_kernel(const float* __restrict__ src, const float* __restrict__ dst,
+                                                        const float* __restrict__ M_inv, const float* __restrict__ bvec,
+                                                        GridDims<3> G, Tiling T, uint8_t* __restrict__ flags) {
+    const int64_t r = tile_ray_at(T, blockIdx.x, threadIdx.x);
+    bool live = false;
+    if (r >= 0) {
+        float sw[3], dw[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            sw[a] = ld_stream(src + r * 3 + a);
+            dw[a] = ld_stream(dst + r * 3 + a);
+        }
+        LaneRay R;
+        lane_setup(R, sw, dw, G, load_affine3(M_inv, bvec));
+        live = R.live;
+    }
+    live = __syncthreads_or(live);
+    if (threadIdx.x == 0) flags[blockIdx.x] = live ? 1 : 0;
+}
+
+// The flagged tile indices in ascending order (the launch order of the full
+// tiling, so a list launch keeps its locality), by one CTA of 1024 threads:
+// per chunk of 1024 flags a warp-ballot and shared-memory prefix count.
+__global__ void __launch_bounds__(1024) compact_tiles_kernel(const uint8_t* __restrict__ flags, int64_t n,
+                                                             int32_t* __restrict__ tiles_out,
+                                                             int64_t* __restrict__ n_out) {
+    __shared__ int warp_base[32];
+    __shared__ int chunk_total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t base = 0;
+    for (int64_t start = 0; start < n; start += 1024) {
+        const int64_t i = start + threadIdx.x;
+        const bool f = i < n && flags[i] != 0;
+        const unsigned bal = __ballot_sync(kFullMask, f);
+        if (lane == 0) warp_base[warp] = __popc(bal);
+        __syncthreads();
+        if (warp == 0) {  // exclusive prefix over the 32 warp counts
+            const int c = warp_base[lane];
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFullMask, incl, o);
+                if (lane >= o) incl += v;
+            }
+            warp_base[lane] = incl - c;
+            if (lane == 31) chunk_total = incl;
+        }
+        __syncthreads();
+        if (f) tiles_out[base + warp_base[warp] + __popc(bal & ((1u << lane) - 1u))] = (int32_t)i;
+        base += chunk_total;
+        __syncthreads();  // warp_base and chunk_total are rewritten by the next chunk
+    }
+    if (threadIdx.x == 0) *n_out = base;
+}
+
 // Bytes of the reproducible adjoint's workspace: a 256-byte-aligned header
 // (per sinogram its max |y| bits and its scale) and an int64 volume per
 // sinogram.
@@ -334,6 +411,47 @@ static int64_t fixed_header_bytes(int64_t batch) { return ((batch * 8 + 255) / 2
 }  // namespace ctlab
 
 using namespace ctlab;
+
+extern "C" int64_t ctlab_tile_count(int64_t n_ray, const ctlab_ray_opts* tiling) {
+    clear_error();
+    if (n_ray < 1) return -1;
+    Tiling T;
+    if (resolve_tiling(tiling, n_ray, T) != CTLAB_OK || T.n_blocks > kMaxGrid) return -1;
+    return T.n_blocks;
+}
+
+extern "C" int ctlab_active_tiles(const float* src, const float* dst, int64_t n_ray, const float* M_inv,
+                                  const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
+                                  const ctlab_ray_opts* tiling, uint8_t* flags, int32_t* tiles_out, int64_t* n_out,
+                                  void* stream) {
+    clear_error();
+    const char* what = "active_tiles";
+    CTLAB_REQUIRE(n_ray >= 1, "%s: n_ray must be >= 1", what);
+    CTLAB_REQUIRE(src && dst && M_inv && b && flags && tiles_out && n_out, "%s: null pointer", what);
+    const int64_t dims[3] = {n_x, n_y, n_z};
+    GridDims<3> G;
+    int64_t nvox = 1, st = 1;
+    for (int a = 0; a < 3; ++a) {
+        CTLAB_REQUIRE(dims[a] >= 1 && dims[a] <= (1 << 22), "%s: grid dimension %d out of range", what, a);
+        nvox *= dims[a];
+    }
+    CTLAB_REQUIRE(nvox < (1LL << 31), "%s: a volume of %lld voxels exceeds 2^31", what, (long long)nvox);
+    for (int a = 2; a >= 0; --a) {
+        G.n[a] = (int)dims[a];
+        G.stride[a] = (int)st;
+        st *= dims[a];
+    }
+    Tiling T;
+    int rc = resolve_tiling(tiling, n_ray, T);
+    if (rc) return rc;
+    CTLAB_REQUIRE(T.n_blocks <= kMaxGrid, "%s: too many tiles", what);
+    cudaStream_t s = as_stream(stream);
+    tile_live_kernel<<<(unsigned)T.n_blocks, T.tile_rows * T.tile_cols, 0, s>>>(src, dst, M_inv, b, G, T, flags);
+    rc = launch_status(what);
+    if (rc) return rc;
+    compact_tiles_kernel<<<1, 1024, 0, s>>>(flags, T.n_blocks, tiles_out, n_out);
+    return launch_status(what);
+}
 
 extern "C" int64_t ctlab_back_project_3d_fixed_workspace_bytes(int64_t batch, int64_t n_x, int64_t n_y,
                                                                int64_t n_z) {
@@ -344,8 +462,8 @@ extern "C" int64_t ctlab_back_project_3d_fixed_workspace_bytes(int64_t batch, in
 extern "C" int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int64_t n_ray, const float* src,
                                            const float* dst, const float* M_inv, const float* b, int64_t n_x,
                                            int64_t n_y, int64_t n_z, float* out, int accumulate,
-                                           const ctlab_ray_opts* tiling, void* workspace, int64_t workspace_bytes,
-                                           void* stream) {
+                                           const ctlab_ray_opts* tiling, const int32_t* tiles, int64_t n_tiles,
+                                           void* workspace, int64_t workspace_bytes, void* stream) {
     clear_error();
     const char* what = "back_project_3d_fixed";
     CTLAB_REQUIRE(batch >= 1 && batch <= 65535, "%s: batch must be in [1, 65535], got %lld", what, (long long)batch);
@@ -389,6 +507,13 @@ extern "C" int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int
         rc = resolve_tiling(tiling, n_ray, T);
         if (rc) return rc;
         CTLAB_REQUIRE(T.n_blocks <= kMaxGrid, "%s: too many rays for one launch", what);
+        if (n_tiles >= 0) {  // only the listed tiles (ctlab_active_tiles); the others add nothing
+            CTLAB_REQUIRE(n_tiles <= T.n_blocks && (n_tiles == 0 || tiles != nullptr),
+                          "%s: bad tile list (%lld tiles of %lld)", what, (long long)n_tiles, (long long)T.n_blocks);
+            T.tiles = tiles;
+            T.n_full = T.n_blocks;
+            T.n_blocks = n_tiles;
+        }
         const int threads = T.tile_rows * T.tile_cols;
         const bool mid = tiling == nullptr || tiling->voxel_rule == CTLAB_VOXEL_MIDPOINT;
         const bool flat = tiling == nullptr || tiling->n_view == 0;
@@ -396,7 +521,9 @@ extern "C" int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int
         const bool small_grid = G.n[0] <= 65536 && G.n[1] <= 65536 && G.n[2] <= 65536;
         const dim3 g((unsigned)T.n_blocks, (unsigned)batch);
         float* o = reinterpret_cast<float*>(sums);
-        if (!flat && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
+        if (T.n_blocks == 0) {
+            // an empty tile list: nothing to walk (the sums stay zero)
+        } else if (!flat && small_grid && (T.tile_rows % 32 == 0 || T.tile_rows == 16) &&
             (walk == CTLAB_WALK_COLUMN || walk == CTLAB_WALK_AUTO)) {
             if (T.tile_rows == 16) {
                 if (mid) siddon3d_fixed_column_kernel<true, 16><<<g, threads, 0, s>>>(sino, o, src, dst, n_ray, M_inv, b, G, nvox, T, scale);
@@ -438,6 +565,30 @@ extern "C" int ctlab_back_project_3d_on_the_fly_ex(const float* sino, int64_t ba
     const int64_t dims[3] = {n_x, n_y, n_z};
     return launch_siddon<3, true>("back_project_3d_on_the_fly", sino, out, batch, dims, src, dst, n_ray, M_inv, b,
                                   accumulate, tiling, stream);
+}
+
+extern "C" int ctlab_forward_project_3d_on_the_fly_tiles(const float* volume, int64_t batch, int64_t n_x,
+                                                         int64_t n_y, int64_t n_z, const float* src, const float* dst,
+                                                         int64_t n_ray, const float* M_inv, const float* b,
+                                                         float* out, const ctlab_ray_opts* tiling,
+                                                         const int32_t* tiles, int64_t n_tiles, void* stream) {
+    clear_error();
+    CTLAB_REQUIRE(n_tiles >= 0, "forward_project_3d_on_the_fly_tiles: n_tiles must be >= 0");
+    const int64_t dims[3] = {n_x, n_y, n_z};
+    return launch_siddon<3, false>("forward_project_3d_on_the_fly_tiles", volume, out, batch, dims, src, dst, n_ray,
+                                   M_inv, b, 0, tiling, stream, nullptr, tiles, n_tiles);
+}
+
+extern "C" int ctlab_back_project_3d_on_the_fly_tiles(const float* sino, int64_t batch, int64_t n_ray,
+                                                      const float* src, const float* dst, const float* M_inv,
+                                                      const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
+                                                      float* out, int accumulate, const ctlab_ray_opts* tiling,
+                                                      const int32_t* tiles, int64_t n_tiles, void* stream) {
+    clear_error();
+    CTLAB_REQUIRE(n_tiles >= 0, "back_project_3d_on_the_fly_tiles: n_tiles must be >= 0");
+    const int64_t dims[3] = {n_x, n_y, n_z};
+    return launch_siddon<3, true>("back_project_3d_on_the_fly_tiles", sino, out, batch, dims, src, dst, n_ray, M_inv,
+                                  b, accumulate, tiling, stream, nullptr, tiles, n_tiles);
 }
 
 extern "C" int ctlab_forward_project_3d_on_the_fly(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,

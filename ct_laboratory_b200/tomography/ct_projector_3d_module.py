@@ -31,6 +31,7 @@ import math
 import torch
 
 from .. import _C
+from .. import _native as N
 from ._common import InverseCache, require_cuda, voxel_diag_len
 from .ct_projector_3d_autograd import CTProjector3DFunction
 from .ct_projector_3d_cuda import back_project_3d_cuda, compute_intersections_3d_cuda
@@ -73,6 +74,7 @@ class CTProjector3DModule(torch.nn.Module):
         self.n_x, self.n_y, self.n_z = int(n_x), int(n_y), int(n_z)
         self.use_compression = use_compression
         self.ray_tiling = ray_tiling
+        self._active = {}  # launch tiling -> (geometry, versions, ActiveRayOpts)
         self._minv = InverseCache()
         # the kernels read raw pointers: keep contiguous float32 copies
         f32 = lambda t: t.to(torch.float32).contiguous()  # noqa: E731
@@ -122,6 +124,32 @@ class CTProjector3DModule(torch.nn.Module):
                     setattr(self, name, t.to(device))
         return self
 
+    def _launch_tiling(self):
+        """ray_tiling with the list of its active tiles (active_tiling_for)."""
+        if self._table()[0] is not None:
+            return self.ray_tiling
+        return self.active_tiling_for(self.ray_tiling)
+
+    def active_tiling_for(self, t):
+        """Launch tiling `t` of this scan with the list of its active tiles
+        (the tiles holding a ray that the walks charge,
+        _native.active_tiling), computed once per geometry and tiling: the
+        on-the-fly launches then skip the tiles whose rays all miss the
+        volume, with the same results.  `t` itself for a flat launch."""
+        if t is None or t.n_view == 0 or not self.src.is_cuda:
+            return t
+        geom = (self.src, self.dst, self.M, self.b)
+        tkey = tuple(getattr(t, f) for f, _ in N.RayOpts._fields_)
+        versions = (tuple(g._version for g in geom), self.n_x, self.n_y, self.n_z)
+        hit = self._active.get(tkey)
+        if hit is not None and hit[1] == versions and all(a is b for a, b in zip(hit[0], geom)):
+            return hit[2]
+        opts = N.active_tiling(t, self.src, self.dst, self.M_inv, self.b, (self.n_x, self.n_y, self.n_z))
+        if len(self._active) >= 8:  # a few launch shapes at most
+            self._active.clear()
+        self._active[tkey] = (geom, versions, opts)
+        return opts
+
     def _panels(self):
         return self.panels if (self.adjoint_mode == "gather" and self._table()[0] is None) else None
 
@@ -145,7 +173,8 @@ class CTProjector3DModule(torch.nn.Module):
         self._ensure_table_device(volume.device)
         t_main, t_start, t_scale = self._table()
         return CTProjector3DFunction.apply(volume, t_main, t_start, t_scale, self.M, self.b, self.src, self.dst,
-                                           self.backend, self.ray_tiling, self.M_inv, self._panels(), self._fixed())
+                                           self.backend, self._launch_tiling(), self.M_inv, self._panels(),
+                                           self._fixed())
 
     def forward_project(self, volume):
         return self.forward(volume)
@@ -163,7 +192,7 @@ class CTProjector3DModule(torch.nn.Module):
                 return back_project_3d_fixed_cuda(sinogram.contiguous(), self.src, self.dst, self.M, self.b, self.n_x,
                                                   self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
             return back_project_3d_cuda(sinogram.contiguous(), tv, self.src, self.dst, self.M, self.b, self.n_x,
-                                        self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
+                                        self.n_y, self.n_z, tiling=self._launch_tiling(), M_inv=self.M_inv)
 
     # -- tvals lifecycle (reference :190-253) ------------------------------
     def save_tvals(self, filePath):

@@ -64,8 +64,10 @@ def back_project_3d_fixed_cuda(sinogram, src, dst, M, b, n_x, n_y, n_z, tiling=N
     elif tuple(out.shape[-3:]) != (n_x, n_y, n_z) or out.numel() != batch * n_x * n_y * n_z or \
             out.dtype != torch.float32 or not out.is_contiguous():
         raise RuntimeError("out must be a contiguous float32 [B, n_x, n_y, n_z] volume")
+    act = getattr(tiling, "active", None)  # a list of active tiles (_native.active_tiling): walk only those
+    tiles, n_tiles = (N.ptr(act[0]), act[1]) if act is not None else (None, -1)
     with torch.cuda.device(sino.device):
         N.call("ctlab_back_project_3d_fixed", N.ptr(sino), batch, n_ray, N.ptr(src), N.ptr(dst), N.ptr(Mi),
-               N.ptr(b), n_x, n_y, n_z, N.ptr(out), int(bool(accumulate)), N.tiling_ref(tiling), N.ptr(workspace),
-               workspace.numel(), N.stream_of(sino))
+               N.ptr(b), n_x, n_y, n_z, N.ptr(out), int(bool(accumulate)), N.tiling_ref(tiling), tiles, n_tiles,
+               N.ptr(workspace), workspace.numel(), N.stream_of(sino))
     return out.reshape(n_x, n_y, n_z) if squeeze and out.dim() == 4 else out

@@ -134,6 +134,35 @@ int ctlab_back_project_3d_on_the_fly_ex(const float* sino, int64_t batch, int64_
                                         int64_t n_y, int64_t n_z, float* out, int accumulate,
                                         const ctlab_ray_opts* tiling, void* stream);
 
+/* Active tiles.  A projector's geometry is fixed, while most of a scan's
+ * rays may miss the volume (about two thirds on a cone-beam scan whose
+ * detector overhangs the volume).  ctlab_active_tiles lists, once, the tiles
+ * of `tiling` (the CTAs of the *_ex launches) that hold at least one ray the
+ * walks charge: a ray is charged only if its end points are finite, its
+ * direction is not degenerate and some of the box lies inside its [0, 1]
+ * (ctlab_forward_project_3d_on_the_fly_ex applies exactly these tests to
+ * every ray).  The *_tiles calls then launch only the listed tiles: the
+ * forward zeroes its output first (every other ray projects to 0), the
+ * adjoint adds nothing for them, so the results are those of the *_ex calls
+ * with the same tiling.  `flags` is device workspace of ctlab_tile_count
+ * bytes, `tiles_out` room for as many int32 entries, `*n_out` (device
+ * memory) receives the count.  No counterpart in the reference, whose
+ * kernels run every ray (src/ct_projector_3d.cu:1018-1049). */
+int64_t ctlab_tile_count(int64_t n_ray, const ctlab_ray_opts* tiling);
+int ctlab_active_tiles(const float* src, const float* dst, int64_t n_ray, const float* M_inv, const float* b,
+                       int64_t n_x, int64_t n_y, int64_t n_z, const ctlab_ray_opts* tiling, uint8_t* flags,
+                       int32_t* tiles_out, int64_t* n_out, void* stream);
+int ctlab_forward_project_3d_on_the_fly_tiles(const float* volume, int64_t batch, int64_t n_x, int64_t n_y,
+                                              int64_t n_z, const float* src, const float* dst, int64_t n_ray,
+                                              const float* M_inv, const float* b, float* out,
+                                              const ctlab_ray_opts* tiling, const int32_t* tiles, int64_t n_tiles,
+                                              void* stream);
+int ctlab_back_project_3d_on_the_fly_tiles(const float* sino, int64_t batch, int64_t n_ray, const float* src,
+                                           const float* dst, const float* M_inv, const float* b, int64_t n_x,
+                                           int64_t n_y, int64_t n_z, float* out, int accumulate,
+                                           const ctlab_ray_opts* tiling, const int32_t* tiles, int64_t n_tiles,
+                                           void* stream);
+
 /*
  * One flat detector panel: a view whose cell centres form an affine grid
  *     dst(ju, jv) = origin + ju * du + jv * dv,   ray = first_ray + jv*v_stride + ju*u_stride
@@ -185,12 +214,14 @@ int ctlab_back_project_3d_gather_ws(const float* sino, int64_t batch, int64_t n_
  * in the reference (its adjoints scatter with float atomicAdd,
  * src/ct_projector_3d.cu:1005).  `workspace` is device memory, 256-byte
  * aligned, of ctlab_back_project_3d_fixed_workspace_bytes bytes (one int64
- * volume per sinogram plus a header); it is cleared here. */
+ * volume per sinogram plus a header); it is cleared here.  `tiles` /
+ * `n_tiles`: a list of active tiles of `tiling` (ctlab_active_tiles) to walk
+ * only those, or NULL / -1 for every tile. */
 int64_t ctlab_back_project_3d_fixed_workspace_bytes(int64_t batch, int64_t n_x, int64_t n_y, int64_t n_z);
 int ctlab_back_project_3d_fixed(const float* sino, int64_t batch, int64_t n_ray, const float* src, const float* dst,
                                 const float* M_inv, const float* b, int64_t n_x, int64_t n_y, int64_t n_z,
-                                float* out, int accumulate, const ctlab_ray_opts* tiling, void* workspace,
-                                int64_t workspace_bytes, void* stream);
+                                float* out, int accumulate, const ctlab_ray_opts* tiling, const int32_t* tiles,
+                                int64_t n_tiles, void* workspace, int64_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------- */
 /* Elementwise steps of a MAP iteration (the reconstruction server)        */

@@ -1,0 +1,91 @@
+"""Active-tile launches (ctlab_active_tiles + the *_tiles entry points).
+
+The tiles listed are those holding a ray the walks charge; launching only
+them must give the full launch's results: the forward bitwise (the same
+walks, and 0 for every ray of a skipped tile), the adjoint to the order of
+its float additions (1e-6 of the maximum), and the reproducible adjoint
+bitwise.  The geometry has a detector much wider and taller than the
+volume's shadow, so most tiles are skipped; the cases cover both voxel
+rules, 32- and 16-row tiles, batches of volumes, and an empty list.  The
+reproducible adjoint runs every tile and accepts the listed tiling.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def cone(rows=32, rule=0, det=(96, 80), n=(24, 20, 16)):
+    from ct_laboratory_b200 import ConeBeam3DProjector
+    return ConeBeam3DProjector(*n, n_view=9, det_nx=det[0], det_ny=det[1], sid=100.0, sdd=150.0, det_spacing=0.8,
+                               voxel_size=0.5, device=torch.device(DEV), tile_rows=rows, voxel_rule=rule)
+
+
+@pytest.mark.parametrize("rows,rule", [(32, 0), (32, 1), (16, 0), (16, 1)])
+def test_tile_list_launches_equal_full_launches(rows, rule):
+    from ct_laboratory_b200 import _C
+    from ct_laboratory_b200 import _native as N
+    p = cone(rows, rule)
+    act = p._launch_tiling()
+    n_all = int(N.lib.ctlab_tile_count(p.src.shape[0], N.tiling_ref(p.ray_tiling)))
+    n_act = act.active[1]
+    assert 0 < n_act < n_all // 2, (n_act, n_all)  # most of the detector misses the volume
+    tiles = act.active[0].cpu().numpy()
+    assert np.all(np.diff(tiles) > 0) and tiles[0] >= 0 and tiles[-1] < n_all  # ascending, in range
+    g = torch.Generator(device=DEV).manual_seed(rows + rule)
+    for batch in (1, 3):
+        x = torch.rand(batch, p.n_x, p.n_y, p.n_z, generator=g, device=DEV)
+        y = torch.rand(batch, p.src.shape[0], generator=g, device=DEV)
+        args = (p.src, p.dst, p.M_inv, p.b)
+        f_full = _C.forward_project_3d_on_the_fly_cuda(x, *args, tiling=p.ray_tiling)
+        f_act = _C.forward_project_3d_on_the_fly_cuda(x, *args, tiling=act)
+        assert torch.equal(f_full, f_act)
+        b_full = _C.back_project_3d_on_the_fly_cuda(y, *args, p.n_x, p.n_y, p.n_z, tiling=p.ray_tiling)
+        b_act = _C.back_project_3d_on_the_fly_cuda(y, *args, p.n_x, p.n_y, p.n_z, tiling=act)
+        assert rel_err(b_act.cpu().numpy(), b_full.cpu().numpy()) < 1e-6
+    # the module's own calls take the list
+    with torch.no_grad():
+        assert torch.equal(p.forward_project(x[0]), f_full[0])
+
+
+def test_tile_lists_follow_the_geometry_and_the_empty_list():
+    from ct_laboratory_b200 import _C
+    from ct_laboratory_b200 import _native as N
+    p = cone()
+    a1 = p._launch_tiling()
+    assert p._launch_tiling() is a1  # cached
+    with torch.no_grad():
+        p.dst[:, 2] += 1000.0  # every ray now passes far above the volume
+    a2 = p._launch_tiling()
+    assert a2 is not a1 and a2.active[1] == 0
+    x = torch.rand(p.n_x, p.n_y, p.n_z, device=DEV)
+    out = _C.forward_project_3d_on_the_fly_cuda(x, p.src, p.dst, p.M_inv, p.b, tiling=a2)
+    assert int(torch.count_nonzero(out)) == 0
+    full = _C.forward_project_3d_on_the_fly_cuda(x, p.src, p.dst, p.M_inv, p.b, tiling=p.ray_tiling)
+    assert int(torch.count_nonzero(full)) == 0
+    # a list longer than the tiling is refused on the host
+    n_all = int(N.lib.ctlab_tile_count(p.src.shape[0], N.tiling_ref(p.ray_tiling)))
+    bogus = torch.zeros(n_all + 1, dtype=torch.int32, device=DEV)
+    o = torch.empty(1, p.src.shape[0], device=DEV)
+    rc = N.lib.ctlab_forward_project_3d_on_the_fly_tiles(N.ptr(x), 1, p.n_x, p.n_y, p.n_z, N.ptr(p.src),
+                                                         N.ptr(p.dst), p.src.shape[0], N.ptr(p.M_inv), N.ptr(p.b),
+                                                         N.ptr(o), N.tiling_ref(p.ray_tiling), N.ptr(bogus),
+                                                         n_all + 1, N.stream_of(x))
+    assert rc != 0
+
+
+def test_reproducible_adjoint_accepts_the_listed_tiling():
+    """The fixed-point adjoint takes the module's launch tiling (it runs
+    every tile) and gives the same bits."""
+    from ct_laboratory_b200.tomography import back_project_3d_fixed_cuda
+    p = cone()
+    act = p._launch_tiling()
+    y = torch.rand(p.src.shape[0], device=DEV)
+    a = back_project_3d_fixed_cuda(y, p.src, p.dst, p.M, p.b, p.n_x, p.n_y, p.n_z, tiling=p.ray_tiling,
+                                   M_inv=p.M_inv)
+    b = back_project_3d_fixed_cuda(y, p.src, p.dst, p.M, p.b, p.n_x, p.n_y, p.n_z, tiling=act, M_inv=p.M_inv)
+    assert torch.equal(a, b)

@@ -157,19 +157,19 @@ def test_fixed_adjoint_without_rays_and_host_errors():
     stream = N.stream_of(out)
     for acc, want in ((1, 7.0), (0, 0.0)):
         N.call("ctlab_back_project_3d_fixed", None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), acc,
-               None, N.ptr(ws), need, stream)
+               None, None, -1, N.ptr(ws), need, stream)
         torch.cuda.synchronize()
         assert bool((out == want).all())
     assert N.lib.ctlab_back_project_3d_fixed_workspace_bytes(0, *n) < 0
     rc = N.lib.ctlab_back_project_3d_fixed(None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
-                                           N.ptr(ws), need - 8, stream)
+                                           None, -1, N.ptr(ws), need - 8, stream)
     assert rc != 0 and b"workspace" in N.lib.ctlab_last_error()
     odd = ws[8:]  # 8 bytes past a 256-byte boundary
     rc = N.lib.ctlab_back_project_3d_fixed(None, 1, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
-                                           N.ptr(odd), need, stream)
+                                           None, -1, N.ptr(odd), need, stream)
     assert rc != 0
     rc = N.lib.ctlab_back_project_3d_fixed(None, 0, 0, None, None, N.ptr(Mi), N.ptr(b), *n, N.ptr(out), 0, None,
-                                           N.ptr(ws), need, stream)
+                                           None, -1, N.ptr(ws), need, stream)
     assert rc != 0 and b"batch" in N.lib.ctlab_last_error()
     fan = FanBeam2DProjector(16, 16, n_view=4, n_det=20, sid=100.0, sdd=150.0, det_spacing=1.0, pixel_size=1.0,
                              device=torch.device(DEV))
