@@ -190,7 +190,7 @@ class CTProjector3DModule(torch.nn.Module):
                                                    self.n_z, self.panels, M_inv=self.M_inv)
             if self._fixed():
                 return back_project_3d_fixed_cuda(sinogram.contiguous(), self.src, self.dst, self.M, self.b, self.n_x,
-                                                  self.n_y, self.n_z, tiling=self.ray_tiling, M_inv=self.M_inv)
+                                                  self.n_y, self.n_z, tiling=self._launch_tiling(), M_inv=self.M_inv)
             return back_project_3d_cuda(sinogram.contiguous(), tv, self.src, self.dst, self.M, self.b, self.n_x,
                                         self.n_y, self.n_z, tiling=self._launch_tiling(), M_inv=self.M_inv)
 

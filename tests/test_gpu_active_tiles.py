@@ -6,8 +6,7 @@ walks, and 0 for every ray of a skipped tile), the adjoint to the order of
 its float additions (1e-6 of the maximum), and the reproducible adjoint
 bitwise.  The geometry has a detector much wider and taller than the
 volume's shadow, so most tiles are skipped; the cases cover both voxel
-rules, 32- and 16-row tiles, batches of volumes, and an empty list.  The
-reproducible adjoint runs every tile and accepts the listed tiling.
+rules, 32- and 16-row tiles, batches of volumes, and an empty list.
 """
 import numpy as np
 import pytest
@@ -78,9 +77,9 @@ def test_tile_lists_follow_the_geometry_and_the_empty_list():
     assert rc != 0
 
 
-def test_reproducible_adjoint_accepts_the_listed_tiling():
-    """The fixed-point adjoint takes the module's launch tiling (it runs
-    every tile) and gives the same bits."""
+def test_reproducible_adjoint_with_a_tile_list_is_bitwise_the_same():
+    """The fixed-point adjoint walking only the listed tiles gives the full
+    launch's bits (integer sums of the same contributions)."""
     from ct_laboratory_b200.tomography import back_project_3d_fixed_cuda
     p = cone()
     act = p._launch_tiling()
