@@ -379,6 +379,16 @@ def run_ours(args, world, rank, local):
     total_ms = max_over_ranks(total_ms, world)
     value = rays_per_step * args.steps / (total_ms / 1e3) / 1e9
 
+    # the launches cover the scan's active tiles (CTProjector3DModule.active_tiling_for)
+    tiles_note = "every tile"
+    local = getattr(proj, "local", proj)
+    if hasattr(local, "_launch_tiling"):
+        t = local._launch_tiling()
+        act = getattr(t, "active", None)
+        if act is not None:
+            from ct_laboratory_b200 import _native as N
+            n_all = int(N.lib.ctlab_tile_count(int(local.src.shape[0]), N.tiling_ref(t)))
+            tiles_note = f"active tiles only: {act[1]} of {n_all} (the rest hold no ray that crosses the volume)"
     peak, peak_src = peaks()
     bytes_per_launch, seg = algorithmic_bytes(w.name, n_ray)
     if args.sharded and bytes_per_launch:
@@ -424,6 +434,7 @@ def run_ours(args, world, rank, local):
                           "tile_rows": args.tile_rows, "block_threads": args.block_threads,
                           "voxel_rule": ["midpoint", "crossing"][args.voxel_rule],
                           "walk": ["auto", "lane", "column"][args.walk],
+                          "tiles": tiles_note,
                           "adjoint": {None: "float atomic scatter", "gather": "voxel gather (reproducible)",
                                       "fixed": "64-bit fixed-point scatter (reproducible)"}[args.deterministic],
                           "parallelism": (f"ray-sharded x{world}: one scan, whole views per rank, NCCL "
