@@ -17,8 +17,37 @@ from __future__ import annotations
 
 import torch
 
+import weakref
+from collections import OrderedDict
+
 from . import _layout
 from . import _native as N
+
+# Active-tile lists of bare calls (no launch hint): keyed by the geometry
+# tensors (weak references plus their versions: a freed tensor's address
+# that comes back with other contents never matches) and by the values of
+# M^-1 and b, which callers such as the reference's wrappers rebuild on
+# every call.  Comparing those 12 values reads them to the host once per
+# call.
+_BARE_TILES = OrderedDict()
+_BARE_TILES_MAX = 8
+
+
+def _bare_active(tiling, src, dst, M_inv, b, dims):
+    if tiling is None or tiling.n_view == 0:
+        return tiling
+    vals = torch.cat([M_inv.reshape(-1), b.reshape(-1)]).cpu()
+    key = (id(src), id(dst), tuple(int(v) for v in dims), tuple(getattr(tiling, f) for f, _ in N.RayOpts._fields_))
+    hit = _BARE_TILES.get(key)
+    if (hit is not None and hit[0]() is src and hit[1]() is dst and hit[2] == (src._version, dst._version)
+            and torch.equal(hit[3], vals)):
+        _BARE_TILES.move_to_end(key)
+        return hit[4]
+    opts = N.active_tiling(tiling, src, dst, M_inv, b, dims)
+    _BARE_TILES[key] = (weakref.ref(src), weakref.ref(dst), (src._version, dst._version), vals, opts)
+    while len(_BARE_TILES) > _BARE_TILES_MAX:
+        _BARE_TILES.popitem(last=False)
+    return opts
 
 __all__ = [
     "compute_intersections_2d", "forward_project_2d_cuda", "back_project_2d_cuda",
@@ -243,14 +272,15 @@ def forward_project_3d_on_the_fly_cuda(volume, src, dst, M_inv, b, tiling=None):
     """src/ct_projector_3d.cu:1018-1049 -> [batch, n_ray].  `tiling` (an
     _native.RayOpts) is an optional launch-shape hint, not in the reference;
     without one the detector layout of src / dst is detected once per
-    geometry (_layout.detect_tiling) and the reference's midpoint voxel rule
-    is used."""
+    geometry (_layout.detect_tiling), the reference's midpoint voxel rule is
+    used, and only the tiles holding a ray that crosses the volume are
+    launched (_bare_active: listed once per geometry)."""
     _check_cuda("inputs must be CUDA", volume, src, dst)
     _f32c("volume", volume)
     _geom(src, dst, M_inv, b, 3)
-    if tiling is None:
-        tiling = _layout.detect_tiling(src, dst)
     batch, (n_x, n_y, n_z) = _vol_shape(volume, 3)
+    if tiling is None:
+        tiling = _bare_active(_layout.detect_tiling(src, dst), src, dst, M_inv, b, (n_x, n_y, n_z))
     n_ray = src.shape[0]
     out = torch.empty((batch, n_ray), device=volume.device, dtype=torch.float32)
     act = getattr(tiling, "active", None)  # a list of the active tiles (_native.active_tiling)
@@ -272,7 +302,7 @@ def back_project_3d_on_the_fly_cuda(sino, src, dst, M_inv, b, n_x, n_y, n_z, til
     _f32c("sinogram", sino)
     _geom(src, dst, M_inv, b, 3)
     if tiling is None:
-        tiling = _layout.detect_tiling(src, dst)
+        tiling = _bare_active(_layout.detect_tiling(src, dst), src, dst, M_inv, b, (n_x, n_y, n_z))
     batch, n_ray = _sino_shape(sino)
     out = torch.empty((batch, n_x, n_y, n_z), device=sino.device, dtype=torch.float32)
     act = getattr(tiling, "active", None)

@@ -88,3 +88,34 @@ def test_reproducible_adjoint_with_a_tile_list_is_bitwise_the_same():
                                    M_inv=p.M_inv)
     b = back_project_3d_fixed_cuda(y, p.src, p.dst, p.M, p.b, p.n_x, p.n_y, p.n_z, tiling=act, M_inv=p.M_inv)
     assert torch.equal(a, b)
+
+
+def test_bare_C_calls_list_their_tiles_and_follow_new_values():
+    """_C calls without a launch hint (the reference's wrappers) launch the
+    detected layout's active tiles: results equal the full launch's, a fresh
+    M^-1 tensor with the same values reuses the list, and new values of b
+    (the volume moved) give a new list and the full launch's results again."""
+    from ct_laboratory_b200 import _C
+    from ct_laboratory_b200 import _layout
+    p = cone(det=(96, 64))  # (the layout detection takes row counts that are multiples of 32)
+    x = torch.rand(1, p.n_x, p.n_y, p.n_z, device=DEV)
+    y = torch.rand(1, p.src.shape[0], device=DEV)
+    full_t = _layout.detect_tiling(p.src, p.dst)
+    assert full_t is not None and full_t.n_view > 0
+    _C._BARE_TILES.clear()
+    for b in (p.b, p.b + torch.tensor([0.0, 0.0, 3.0], device=DEV)):
+        b = b.contiguous()
+        Mi = torch.inverse(p.M).contiguous()
+        f = _C.forward_project_3d_on_the_fly_cuda(x, p.src, p.dst, Mi, b)
+        a = _C.back_project_3d_on_the_fly_cuda(y, p.src, p.dst, Mi, b, p.n_x, p.n_y, p.n_z)
+        f_full = _C.forward_project_3d_on_the_fly_cuda(x, p.src, p.dst, Mi, b, tiling=full_t)
+        a_full = _C.back_project_3d_on_the_fly_cuda(y, p.src, p.dst, Mi, b, p.n_x, p.n_y, p.n_z, tiling=full_t)
+        assert torch.equal(f, f_full)
+        assert rel_err(a.cpu().numpy(), a_full.cpu().numpy()) < 1e-6
+        opts = next(reversed(_C._BARE_TILES.values()))[4]
+        assert opts.active is not None and opts.active[1] > 0
+        # a fresh M^-1 with the same values: the same list
+        n_entries = len(_C._BARE_TILES)
+        _C.forward_project_3d_on_the_fly_cuda(x, p.src, p.dst, torch.inverse(p.M).contiguous(), b)
+        assert len(_C._BARE_TILES) == n_entries and next(reversed(_C._BARE_TILES.values()))[4] is opts
+    assert len(_C._BARE_TILES) == 1  # new values replaced the entry (same key, new contents)

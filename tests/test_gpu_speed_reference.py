@@ -77,6 +77,17 @@ def test_cone256_speed_and_parity_vs_reference_cuda(ref):
         t_fwd = _events_ms(lambda: proj.forward_project(x), 5, flush)
         t_adj = _events_ms(lambda: proj.back_project(y), 5, flush)
     ours_rate = n_ray / ((t_fwd + t_adj) / 1e3)
+    # the same scan through the bare _C calls the reference's wrappers make
+    # (no launch hint, a fresh M^-1 per call)
+    with torch.no_grad():
+        for _ in range(2):
+            _C.forward_project_3d_on_the_fly_cuda(x, proj.src, proj.dst, torch.inverse(proj.M).contiguous(), proj.b)
+            _C.back_project_3d_on_the_fly_cuda(y, proj.src, proj.dst, torch.inverse(proj.M).contiguous(), proj.b, *w.n)
+        c_fwd = _events_ms(lambda: _C.forward_project_3d_on_the_fly_cuda(x, proj.src, proj.dst,
+                                                                         torch.inverse(proj.M).contiguous(), proj.b), 3, flush)
+        c_adj = _events_ms(lambda: _C.back_project_3d_on_the_fly_cuda(y, proj.src, proj.dst, torch.inverse(proj.M).contiguous(),
+                                                                      proj.b, *w.n), 3, flush)
+    c_rate = n_ray / ((c_fwd + c_adj) / 1e3)
 
     # the sample: whole views, contiguous in the [view][v][u] ray order
     per_view = w.det_nx * w.det_ny
@@ -116,7 +127,8 @@ def test_cone256_speed_and_parity_vs_reference_cuda(ref):
     e_b = max(e[1] for e in errs.values())
 
     res = {"workload": "cone256", "n_ray": n_ray, "ours_ms_fwd": t_fwd, "ours_ms_adj": t_adj,
-           "ours_grays_s": ours_rate / 1e9, "ref_sample_views": list(SAMPLE_VIEWS), "ref_sample_rays": n_s,
+           "ours_grays_s": ours_rate / 1e9, "c_api_ms_fwd": c_fwd, "c_api_ms_adj": c_adj,
+           "c_api_grays_s": c_rate / 1e9, "ref_sample_views": list(SAMPLE_VIEWS), "ref_sample_rays": n_s,
            "ref_ms_fwd_sample": r_fwd, "ref_ms_adj_sample": r_adj, "ref_grays_s": ref_rate / 1e9,
            "ref_ms_fwd_full_extrapolated": r_fwd * n_ray / n_s, "ref_ms_adj_full_extrapolated": r_adj * n_ray / n_s,
            "speedup": ratio, "parity_fwd_rel": e_f, "parity_adj_rel": e_b, "parity_by_path": errs}
