@@ -109,6 +109,12 @@ class CTProjector3DModule(torch.nn.Module):
                 self.tvals_full = full
             self.precomputed_intersections = True
 
+    def __getstate__(self):
+        # the active-tile lists are device state rebuilt on first use: not copied or pickled
+        state = dict(self.__dict__)
+        state["_active"] = {}
+        return state
+
     # -- geometry helpers -------------------------------------------------
     @property
     def M_inv(self) -> torch.Tensor:

@@ -35,3 +35,24 @@ def test_batch_workload_is_seeded_and_in_range():
             assert w.sources[0] <= d["sources"] <= w.sources[1] and d["views"] == d["sources"] * d["frames"]
         else:
             assert w.views[0] <= d["views"] <= w.views[1]
+
+
+def test_projector_module_copies_without_its_tile_lists():
+    """A 3-D projector module deep-copies and pickles; its cached
+    active-tile lists (device state) are left behind and rebuilt on use."""
+    import copy
+    import pickle
+
+    import torch
+
+    from ct_laboratory_b200 import _native as N
+    from ct_laboratory_b200.tomography import CTProjector3DModule
+    src = torch.zeros(4, 3)
+    dst = torch.ones(4, 3)
+    m = CTProjector3DModule(2, 2, 2, torch.eye(3), torch.zeros(3), src, dst, device=torch.device("cpu"))
+    opts = N.ActiveRayOpts()
+    opts.active = (torch.zeros(3, dtype=torch.int32), 3)
+    m._active[("key",)] = ((m.src, m.dst, m.M, m.b), (0,), opts)
+    for c in (copy.deepcopy(m), pickle.loads(pickle.dumps(m))):
+        assert c._active == {} and torch.equal(c.src, m.src)
+    assert len(m._active) == 1
