@@ -14,8 +14,10 @@ as they arrive:
 * continuous batching: every tick runs one MAP iteration of every active
   job, with ONE batched forward launch and ONE batched adjoint launch for
   all of them (``ScanBatch`` over the jobs' own buffers, uneven sizes and
-  view counts in one persistent launch); the Poisson residual, smoothness
-  prior and update are applied per job.  Jobs join and leave between ticks,
+  view counts; the per-scan launches of large scans cover each scan's active
+  tiles); the Poisson residual, smoothness prior and update are applied per
+  job by three fused kernels (ctlab_map_poisson_residual,
+  ctlab_map_smoothness_step).  Jobs join and leave between ticks,
   so requests that arrive while others run start as soon as memory and a
   slot free up, and their projector work overlaps with the others' in the
   same launches.
