@@ -11,12 +11,13 @@ as they arrive:
   jobs already running;
 * state on the device: an admitted job's geometry, measurements, estimate
   and work buffers stay resident until it finishes;
-* continuous batching: every tick runs one MAP iteration of every active
-  job, with ONE batched forward launch and ONE batched adjoint launch for
-  all of them (``ScanBatch`` over the jobs' own buffers, uneven sizes and
-  view counts; the per-scan launches of large scans cover each scan's active
-  tiles); the Poisson residual, smoothness prior and update are applied per
-  job by three fused kernels (ctlab_map_poisson_residual,
+* continuous batching: every tick runs one MAP iteration of every selected
+  job, with one batched forward and one batched adjoint pass over all of
+  them (``ScanBatch`` over the jobs' own buffers, uneven sizes and view
+  counts: one persistent launch per direction for small scans, one launch
+  per scan over its active tiles for scans that fill the GPU alone); the
+  Poisson residual, smoothness prior and update are applied per job by
+  three fused kernels (ctlab_map_poisson_residual,
   ctlab_map_smoothness_step).  Jobs join and leave between ticks,
   so requests that arrive while others run start as soon as memory and a
   slot free up, and their projector work overlaps with the others' in the
