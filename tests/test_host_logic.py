@@ -56,3 +56,37 @@ def test_projector_module_copies_without_its_tile_lists():
     for c in (copy.deepcopy(m), pickle.loads(pickle.dumps(m))):
         assert c._active == {} and torch.equal(c.src, m.src)
     assert len(m._active) == 1
+
+
+def test_bare_call_tile_cache_keys(monkeypatch):
+    """The active-tile cache of bare _C calls hits only for the same geometry
+    tensors at the same versions with the same M^-1 and b values: a fresh
+    M^-1 tensor with equal values hits; changed values, an in-place edit of
+    the rays or a new ray tensor miss.  (The device work of the list is
+    replaced by a counter here.)"""
+    import torch
+
+    from ct_laboratory_b200 import _C
+    from ct_laboratory_b200 import _native as N
+    calls = []
+
+    def fake(t, src, dst, M_inv, b, dims):
+        calls.append(1)
+        return ("list", len(calls))
+
+    monkeypatch.setattr(N, "active_tiling", fake)
+    _C._BARE_TILES.clear()
+    t = N.tiling(2, 32, 4, 128, 4, 1, tile_rows=32, block_threads=128)
+    src, dst = torch.rand(256, 3), torch.rand(256, 3)
+    Mi, b = torch.eye(3), torch.zeros(3)
+    first = _C._bare_active(t, src, dst, Mi, b, (8, 8, 8))
+    assert _C._bare_active(t, src, dst, torch.eye(3), b.clone(), (8, 8, 8)) is first and len(calls) == 1
+    assert _C._bare_active(t, src, dst, Mi, b + 1.0, (8, 8, 8)) != first and len(calls) == 2
+    src.add_(0.0)  # an in-place edit bumps the version
+    assert len(calls) == 2 and _C._bare_active(t, src, dst, Mi, b + 1.0, (8, 8, 8)) and len(calls) == 3
+    other = src.clone()
+    _C._bare_active(t, other, dst, Mi, b + 1.0, (8, 8, 8))
+    assert len(calls) == 4
+    assert _C._bare_active(None, src, dst, Mi, b, (8, 8, 8)) is None
+    assert _C._bare_active(N.flat_opts(), src, dst, Mi, b, (8, 8, 8)).n_view == 0  # flat launches carry no list
+    _C._BARE_TILES.clear()
